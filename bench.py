@@ -1,0 +1,480 @@
+"""Benchmark driver: batched factor-and-solve throughput on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+Prints ONE JSON line on rank 0.  A "step" is one pass of the hot path over one batch of
+synthetic input already resident in HBM (value); "e2e" repeats it through the public C ABI
+with the inputs copied from pinned host memory and the solutions read back every step.
+
+Workloads (synthetic inputs with the shapes and value distributions of the reference
+configurations; no dataset is involved):
+  gesv_n256   n=256, batch 2048, nrhs 1, A = U diag(s) V' with cond log-uniform in
+              [1e1, 1e6], b ~ U[-1,1]; dgetrf_strided_batched + dgetrs_strided_batched
+              (plain FP64).  Metric: solves/s.
+  getrf_n32   n=32, lda 32, batch 1000, nrhs 1, U[-1,1] from seed 0: dgetrf + dgetrs.
+  potrf_n64   n=64, batch 20000, nrhs 4, A = G G' + n I: dpotrf + dpotrs.
+Inputs are larger than L2 (126 MB) for gesv_n256 and potrf_n64; getrf_n32 (8 MB) rotates
+through 24 distinct copies of the batch so each step reads cold data.
+
+Multi-GPU: the batch members are independent, so every rank runs its own full batch
+(weak scaling, no collective on the data path); the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="gesv_n256",
+                   choices=["gesv_n256", "getrf_n32", "potrf_n64"])
+    p.add_argument("--cpu-seconds", type=float, default=12.0,
+                   help="target CPU time of the bounded CPU-baseline sample")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------- peaks
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "bf16_tflops": d.get("bf16_tflops", 1590.0),
+                "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- inputs
+def make_cond_matrices(torch, n, bc, seed, device, lo=1.0, hi=6.0):
+    """A = U diag(s) V' with U, V from QR of Gaussians and s log-spaced from 1 to 1/kappa,
+    log10(kappa) ~ U[lo, hi] per member.  Generated on the device in chunks."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    A = torch.empty(bc, n, n, dtype=torch.float64, device=device)
+    chunk = 256
+    for c0 in range(0, bc, chunk):
+        c1 = min(bc, c0 + chunk)
+        m = c1 - c0
+        U, _ = torch.linalg.qr(torch.randn(m, n, n, generator=g, device=device,
+                                           dtype=torch.float64))
+        V, _ = torch.linalg.qr(torch.randn(m, n, n, generator=g, device=device,
+                                           dtype=torch.float64))
+        lk = lo + (hi - lo) * torch.rand(m, 1, generator=g, device=device, dtype=torch.float64)
+        t = torch.linspace(0, 1, n, device=device, dtype=torch.float64)[None, :]
+        s = torch.pow(10.0, -lk * t)
+        A[c0:c1] = (U * s[:, None, :]) @ V.transpose(1, 2)
+    return A
+
+
+def colmajor(torch, A):
+    """(bc, m, n) row-major torch tensor -> contiguous buffer whose member b is the
+    column-major m x n matrix (lda = m)."""
+    return A.transpose(1, 2).contiguous()
+
+
+# ----------------------------------------------------------------------------- workloads
+class Workload:
+    pass
+
+
+def build_workload(name, torch, rs, dev, handle):
+    w = Workload()
+    w.name = name
+    if name == "gesv_n256":
+        n, bc, nrhs = 256, 2048, 1
+        A = make_cond_matrices(torch, n, bc, seed=2, device=dev)
+        g = torch.Generator(device=dev)
+        g.manual_seed(3)
+        B = torch.rand(bc, n, nrhs, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+        w.A0 = colmajor(torch, A)            # pristine copy, column-major members
+        w.B0 = colmajor(torch, B)
+        w.Arow = A                           # for residual checks
+        w.Brow = B
+        w.n, w.bc, w.nrhs = n, bc, nrhs
+        w.metric = "batched solves/s at FP64 backward err <=1e-13 (plain FP64 getrf+getrs)"
+        w.unit = "solves/s"
+        w.dtype = "f64"
+        w.config = {"workload": "plain dgetrf+dgetrs strided_batched, n=256, batch=2048, nrhs=1, "
+                               "cond log-uniform [1e1,1e6]", "n": n, "batch": bc, "nrhs": nrhs,
+                    "l2": "inputs 1 GiB > L2 (126 MB); A restored from a pristine copy between "
+                          "steps outside the timed events"}
+        w.flops_per_unit = 2.0 * n ** 3 / 3 + 2.0 * n * n * nrhs
+        w.bytes_per_unit_getrf = 2 * n * n * 8 + 4 * n + 4
+        w.dominant = "getrf_cta_kernel"
+        w.launches_per_step = 2
+    elif name == "getrf_n32":
+        n, bc, nrhs = 32, 1000, 1
+        rng = np.random.default_rng(0)
+        A = torch.from_numpy(rng.uniform(-1, 1, (bc, n, n))).to(dev)
+        B = torch.from_numpy(rng.uniform(-1, 1, (bc, n, nrhs))).to(dev)
+        w.A0 = colmajor(torch, A)
+        w.B0 = colmajor(torch, B)
+        w.Arow, w.Brow = A, B
+        w.n, w.bc, w.nrhs = n, bc, nrhs
+        w.metric = "batched solves/s (plain FP64 getrf+getrs, n=32)"
+        w.unit = "solves/s"
+        w.dtype = "f64"
+        w.rotate = 24
+        w.config = {"workload": "plain dgetrf+dgetrs strided_batched, n=32, lda=32, batch=1000, "
+                               "nrhs=1, U[-1,1] seed 0", "n": n, "batch": bc, "nrhs": nrhs,
+                    "l2": "24 distinct copies of the 8 MB batch rotated (192 MB > L2)"}
+        w.flops_per_unit = 2.0 * n ** 3 / 3 + 2.0 * n * n * nrhs
+        w.bytes_per_unit_getrf = 2 * n * n * 8 + 4 * n + 4
+        w.dominant = "getrf_warp_kernel"
+        w.launches_per_step = 2
+    elif name == "potrf_n64":
+        n, bc, nrhs = 64, 20000, 4
+        g = torch.Generator(device=dev)
+        g.manual_seed(1)
+        G = torch.randn(bc, n, n, generator=g, device=dev, dtype=torch.float64)
+        A = G @ G.transpose(1, 2) + n * torch.eye(n, device=dev, dtype=torch.float64)
+        del G
+        B = torch.randn(bc, n, nrhs, generator=g, device=dev, dtype=torch.float64)
+        w.A0 = colmajor(torch, A)
+        w.B0 = colmajor(torch, B)
+        w.Arow, w.Brow = A, B
+        w.n, w.bc, w.nrhs = n, bc, nrhs
+        w.metric = "batched SPD solves/s (FP64 potrf+potrs, n=64)"
+        w.unit = "solves/s"
+        w.dtype = "f64"
+        w.config = {"workload": "dpotrf+dpotrs strided_batched lower, n=64, batch=20000, nrhs=4, "
+                               "A = G G' + n I", "n": n, "batch": bc, "nrhs": nrhs,
+                    "l2": "inputs 655 MB > L2; A restored between steps outside the timed events"}
+        w.flops_per_unit = n ** 3 / 3.0 + n * n / 2.0 + n / 6.0 + 2.0 * n * n * nrhs
+        w.bytes_per_unit_getrf = 2 * (n * (n + 1) // 2) * 8 + 4  # triangle read+write + info
+        w.dominant = "potrf_cta_kernel"
+        w.launches_per_step = 2
+    else:
+        raise ValueError(name)
+    return w
+
+
+def run_ours(w, torch, rs, dev, handle, steps, warmup):
+    n, bc, nrhs = w.n, w.bc, w.nrhs
+    rot = getattr(w, "rotate", 1)
+    As = [w.A0.clone() for _ in range(rot)]
+    Bs = [w.B0.clone() for _ in range(rot)]
+    ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
+    info = torch.zeros(bc, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    h = handle.value
+
+    def launch(A, B):
+        if w.name == "potrf_n64":
+            st = rs.call("rocsolver_dpotrf_strided_batched", h, rs.FILL_LOWER, n, rs.ptr(A), n,
+                         n * n, rs.ptr(info), bc)
+            rs.check(st, "potrf")
+            st = rs.call("rocsolver_dpotrs_strided_batched", h, rs.FILL_LOWER, n, nrhs, rs.ptr(A),
+                         n, n * n, rs.ptr(B), n, n * nrhs, bc)
+            rs.check(st, "potrs")
+        else:
+            st = rs.call("rocsolver_dgetrf_strided_batched", h, n, n, rs.ptr(A), n, n * n,
+                         rs.ptr(ipiv), n, rs.ptr(info), bc)
+            rs.check(st, "getrf")
+            st = rs.call("rocsolver_dgetrs_strided_batched", h, rs.OP_N, n, nrhs, rs.ptr(A), n,
+                         n * n, rs.ptr(ipiv), n, rs.ptr(B), n, n * nrhs, bc)
+            rs.check(st, "getrs")
+
+    def restore(i):
+        As[i].copy_(w.A0)
+        Bs[i].copy_(w.B0)
+
+    for i in range(warmup):
+        restore(i % rot)
+        launch(As[i % rot], Bs[i % rot])
+    torch.cuda.synchronize()
+    for i in range(rot):
+        restore(i)
+    torch.cuda.synchronize()
+    # timed region: per-step event pairs on the launching stream; the restore copies
+    # (needed because the factorisation is in place) sit between the pairs
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    kev = []
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    time.sleep(0.3)
+    for i in range(steps):
+        j = i % rot
+        if rot == 1 or (i > 0 and j == 0):
+            for r in range(rot):
+                restore(r)
+        ev[i][0].record(stream)
+        launch(As[j], Bs[j])
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    # kernel-only timing of the dominant factorisation kernel (same stream)
+    fev = []
+    for i in range(min(steps, 10)):
+        restore(0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        if w.name == "potrf_n64":
+            rs.check(rs.call("rocsolver_dpotrf_strided_batched", h, rs.FILL_LOWER, n,
+                             rs.ptr(As[0]), n, n * n, rs.ptr(info), bc), "potrf")
+        else:
+            rs.check(rs.call("rocsolver_dgetrf_strided_batched", h, n, n, rs.ptr(As[0]), n,
+                             n * n, rs.ptr(ipiv), n, rs.ptr(info), bc), "getrf")
+        b.record(stream)
+        fev.append((a, b))
+    torch.cuda.synchronize()
+    fact_ms = statistics.median([a.elapsed_time(b) for a, b in fev])
+    # correctness of the last timed step: backward error per member, on the device
+    restore(0)
+    launch(As[0], Bs[0])
+    X = Bs[0].view(bc, nrhs, n).transpose(1, 2)
+    R = torch.bmm(w.Arow, X) - w.Brow
+    num = R.abs().sum(2).amax(1)
+    den = w.Arow.abs().sum(2).amax(1) * X.abs().sum(2).amax(1) + w.Brow.abs().sum(2).amax(1)
+    berr = (num / den)
+    info_h = info.cpu().numpy()
+    return {"step_ms": step_ms, "fact_ms": fact_ms, "clocks": clocks,
+            "berr_max": float(berr.max()), "berr_frac_1e13": float((berr <= 1e-13).double().mean()),
+            "info_nonzero": int((info_h != 0).sum())}
+
+
+def run_e2e(w, torch, rs, dev, handle, steps):
+    """Same step through the public C ABI with host buffers: pinned A and B copied H2D,
+    factor + solve, solutions and info copied D2H, every step."""
+    n, bc, nrhs = w.n, w.bc, w.nrhs
+    hA = w.A0.cpu().pin_memory()
+    hB = w.B0.cpu().pin_memory()
+    hX = torch.empty_like(hB).pin_memory()
+    hI = torch.empty(bc, dtype=torch.int32).pin_memory()
+    dA = torch.empty_like(w.A0)
+    dB = torch.empty_like(w.B0)
+    ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
+    info = torch.zeros(bc, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    h = handle.value
+
+    def step():
+        dA.copy_(hA, non_blocking=True)
+        dB.copy_(hB, non_blocking=True)
+        if w.name == "potrf_n64":
+            rs.check(rs.call("rocsolver_dposv_strided_batched", h, rs.FILL_LOWER, n, nrhs,
+                             rs.ptr(dA), n, n * n, rs.ptr(dB), n, n * nrhs, rs.ptr(info), bc),
+                     "posv")
+        else:
+            rs.check(rs.call("rocsolver_dgetrf_strided_batched", h, n, n, rs.ptr(dA), n, n * n,
+                             rs.ptr(ipiv), n, rs.ptr(info), bc), "getrf")
+            rs.check(rs.call("rocsolver_dgetrs_strided_batched", h, rs.OP_N, n, nrhs, rs.ptr(dA),
+                             n, n * n, rs.ptr(ipiv), n, rs.ptr(dB), n, n * nrhs, bc), "getrs")
+        hX.copy_(dB, non_blocking=True)
+        hI.copy_(info, non_blocking=True)
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k = max(3, min(steps, 10))
+    a.record(stream)
+    for _ in range(k):
+        step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / k
+    return {"ms": ms, "h2d": hA.numel() * 8 + hB.numel() * 8, "d2h": hX.numel() * 8 + bc * 4}
+
+
+# ----------------------------------------------------------------------------- CPU side
+def cpu_sample(w, target_s):
+    """Time the oracle (unblocked LAPACK-algorithm restatement, one call per member,
+    members split over all host threads) on a bounded sample of the same inputs."""
+    import oracle
+    n, nrhs = w.n, w.nrhs
+    Ah = w.A0.cpu().numpy()
+    Bh = w.B0.cpu().numpy()
+    threads = oracle.nthreads_default()
+
+    def run(cnt):
+        cnt = min(cnt, w.bc)
+        A = Ah[:cnt].reshape(-1).copy()
+        B = Bh[:cnt].reshape(-1).copy()
+        ipiv = np.zeros(cnt * n, np.int32)
+        info = np.zeros(cnt, np.int32)
+        t0 = time.perf_counter()
+        if w.name == "potrf_n64":
+            oracle.posv(False, n, nrhs, A, n, n * n, B, n, n * nrhs, info, cnt, nthreads=threads)
+        else:
+            oracle.getrf(n, n, A, n, n * n, ipiv, n, info, cnt, nthreads=threads)
+            oracle.getrs(0, n, nrhs, A, n, n * n, ipiv, n, B, n, n * nrhs, cnt, nthreads=threads)
+        return time.perf_counter() - t0, cnt
+
+    t, c = run(max(threads, 8))
+    want = int(c * max(1.0, target_s / max(t, 1e-6)))
+    want = max(c, min(want, w.bc))
+    t, c = run(want)
+    return {"value": c / t, "unit": w.unit, "cores": threads, "kind": "port",
+            "sample": f"{c} of {w.bc} members of the same batch, oracle/oracle.c "
+                      f"(unblocked LAPACK getf2/getrs or potf2/potrs restatement), "
+                      f"{threads} pthreads, {t:.1f} s"}
+
+
+# ----------------------------------------------------------------------------- main
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return main_reference(args, rank, world)
+
+    import torch
+    import rocsolver_b200 as rs
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    handle = rs.Handle(torch.cuda.current_stream().cuda_stream)
+    w = build_workload(args.workload, torch, rs, dev, handle)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    res = run_ours(w, torch, rs, dev, handle, args.steps, args.warmup)
+    total_ms = sum(res["step_ms"])
+    if pg:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    e2e = run_e2e(w, torch, rs, dev, handle, args.steps)
+    if pg:
+        t = torch.tensor([e2e["ms"]], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e["ms"] = float(t.item())
+    ms_per_step = total_ms / args.steps
+    units = w.bc * world
+    value = units / (ms_per_step / 1e3)
+    peaks = load_peaks()
+    fact_s = res["fact_ms"] / 1e3
+    achieved_gbs = w.bytes_per_unit_getrf * w.bc / fact_s / 1e9
+    line = {
+        "metric": w.metric, "value": value, "unit": w.unit, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
+        "data": "synthetic (seeded, generated on device)", "config": w.config,
+        "gpu_launches": w.launches_per_step * args.steps,
+        "e2e": {"value": units / (e2e["ms"] / 1e3), "unit": w.unit,
+                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
+        "roofline": {"bound": "hbm", "kernel": w.dominant, "achieved": achieved_gbs,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": None,
+                     "peak_source": peaks["source"],
+                     "kernel_ms": res["fact_ms"],
+                     "fp64_tflops": w.flops_per_unit * w.bc / fact_s / 1e12},
+        "clocks": res["clocks"],
+        "accuracy": {"backward_err_max": res["berr_max"],
+                     "frac_backward_err_le_1e-13": res["berr_frac_1e13"],
+                     "info_nonzero": res["info_nonzero"]},
+    }
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_sample(w, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    handle.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main_reference(args, rank, world):
+    """Reference arm: the reference's own path is HIP/rocBLAS for AMD GPUs and cannot run
+    here; its CPU implementation of the path is host LAPACK, restated by the oracle.  Rank 0
+    times the oracle on the host cores over a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    import torch
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
+    w = build_workload(args.workload, torch, None, dev, None)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(w, max(1.0, args.cpu_seconds / max(1, args.steps)))
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = statistics.median(vals)
+    line = {"metric": w.metric, "value": v, "unit": w.unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
+            "data": "synthetic (seeded)", "config": w.config, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": w.unit, "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": w.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,587 @@
+/* rocsolver-b200: B200 (sm_100a) implementation of rocSOLVER's batched dense
+ * LU / Cholesky factor-and-solve path, exported under the reference's C ABI.
+ *
+ * The types below restate the subset of rocBLAS's public types that the
+ * rocSOLVER prototypes use (library/src/include/rocblas.hpp:17-36 names the
+ * status codes; rocsolver-extra-types.h:13-20 the layer flags).  The numeric
+ * values are rocBLAS's public-header values so that a program compiled against
+ * the real headers passes the same integers.
+ *
+ * Conventions (identical to the reference, library/include/rocsolver/rocsolver-functions.h):
+ *   - matrices are column-major, element (i,j) at A[i + j*lda];
+ *   - strided batches: member b starts at A + b*strideA (strides in elements, int64);
+ *   - pointer-array batches: member b is A[b] (device array of device pointers);
+ *   - ipiv is 1-based, ipiv[b*strideP + k] = row swapped with row k+1;
+ *   - info[b] = 0 on success, k > 0 when U(k,k) is exactly zero (getrf) or the
+ *     leading minor of order k is not positive (potrf);
+ *   - every call is asynchronous on the handle's stream and never synchronises,
+ *     so sequences of calls can be captured into a CUDA graph.
+ * All array arguments are device memory owned by the caller.
+ */
+#ifndef ROCSOLVER_B200_ROCSOLVER_H
+#define ROCSOLVER_B200_ROCSOLVER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define ROCSOLVER_EXPORT
+#else
+#define ROCSOLVER_EXPORT __attribute__((visibility("default")))
+#endif
+
+/* ---- rocBLAS shim types ------------------------------------------------ */
+typedef int32_t rocblas_int;
+typedef int64_t rocblas_stride;
+typedef struct _rocblas_handle* rocblas_handle;
+typedef uint32_t rocblas_layer_mode_flags;
+
+typedef enum rocblas_status_
+{
+    rocblas_status_success = 0,
+    rocblas_status_invalid_handle = 1,
+    rocblas_status_not_implemented = 2,
+    rocblas_status_invalid_pointer = 3,
+    rocblas_status_invalid_size = 4,
+    rocblas_status_memory_error = 5,
+    rocblas_status_internal_error = 6,
+    rocblas_status_perf_degraded = 7,
+    rocblas_status_size_query_mismatch = 8,
+    rocblas_status_size_increased = 9,
+    rocblas_status_size_unchanged = 10,
+    rocblas_status_invalid_value = 11,
+    rocblas_status_continue = 12,
+    rocblas_status_check_numerics_fail = 13
+} rocblas_status;
+
+typedef enum rocblas_operation_
+{
+    rocblas_operation_none = 111,
+    rocblas_operation_transpose = 112,
+    rocblas_operation_conjugate_transpose = 113
+} rocblas_operation;
+
+typedef enum rocblas_fill_
+{
+    rocblas_fill_upper = 121,
+    rocblas_fill_lower = 122,
+    rocblas_fill_full = 123
+} rocblas_fill;
+
+/* ---- handle shim ---------------------------------------------------------
+ * A handle is {CUDA stream, device workspace, size-query state}.  Creating a
+ * handle makes no CUDA call; the workspace is allocated on first need (or is
+ * supplied by the user with rocblas_set_workspace).  Semantics follow the
+ * rocBLAS memory model exercised by clients/gtest/memory_model_gtest.cpp:54-170:
+ * 32 MiB nominal reservation, ROCBLAS_DEVICE_MEMORY_SIZE makes the size
+ * user-fixed, and a size query returns size_increased/size_unchanged instead
+ * of computing. */
+ROCSOLVER_EXPORT rocblas_status rocblas_create_handle(rocblas_handle* handle);
+ROCSOLVER_EXPORT rocblas_status rocblas_destroy_handle(rocblas_handle handle);
+/* stream is a cudaStream_t passed as void* (0 = legacy default stream) */
+ROCSOLVER_EXPORT rocblas_status rocblas_set_stream(rocblas_handle handle, void* stream);
+ROCSOLVER_EXPORT rocblas_status rocblas_get_stream(rocblas_handle handle, void** stream);
+ROCSOLVER_EXPORT rocblas_status rocblas_start_device_memory_size_query(rocblas_handle handle);
+ROCSOLVER_EXPORT rocblas_status rocblas_stop_device_memory_size_query(rocblas_handle handle,
+                                                                      size_t* size);
+ROCSOLVER_EXPORT int rocblas_is_device_memory_size_query(rocblas_handle handle);
+ROCSOLVER_EXPORT int rocblas_is_managing_device_memory(rocblas_handle handle);
+ROCSOLVER_EXPORT rocblas_status rocblas_get_device_memory_size(rocblas_handle handle,
+                                                               size_t* size);
+/* size 0 returns to library-managed memory; otherwise allocates exactly size bytes */
+ROCSOLVER_EXPORT rocblas_status rocblas_set_device_memory_size(rocblas_handle handle,
+                                                               size_t size);
+/* user-owned device workspace (addr may be NULL with size 0 to return to managed mode) */
+ROCSOLVER_EXPORT rocblas_status rocblas_set_workspace(rocblas_handle handle, void* addr,
+                                                      size_t size);
+
+/* library version, mirrors library/src/common/buildinfo.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_get_version_string(char* buf, size_t len);
+ROCSOLVER_EXPORT rocblas_status rocsolver_get_version_string_size(size_t* len);
+
+/* ---- hot path: LU / Cholesky factor and solve ---------------------------
+ * Each prototype keeps the reference's argument order and meaning exactly;
+ * the comment names the reference declaration it replaces
+ * (library/include/rocsolver/rocsolver-functions.h) and its implementation
+ * file (library/src/lapack/).  Argument checks follow the reference order:
+ * invalid_handle, invalid_value (enums), invalid_size, [size query],
+ * invalid_pointer, then quick return. */
+/* replaces rocsolver-functions.h:5139-5155 / lapack/roclapack_getrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrf(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:5227-5247 / lapack/roclapack_getrf_batched.cpp:96-124 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrf_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    float* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:5329-5349 / lapack/roclapack_getrf_strided_batched.cpp:94-122 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrf_strided_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:4609-4622 / lapack/roclapack_getrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrf_npvt(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:4688-4702 / lapack/roclapack_getrf_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrf_npvt_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    float* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:4775-4790 / lapack/roclapack_getrf_strided_batched.cpp:154-208 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrf_npvt_strided_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8562-8580 / lapack/roclapack_getrs.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrs(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_int* ipiv,
+    float* B,
+    const rocblas_int ldb);
+
+/* replaces rocsolver-functions.h:8657-8680 / lapack/roclapack_getrs_batched.cpp:75 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrs_batched(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* const A[],
+    const rocblas_int lda,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    float* const B[],
+    const rocblas_int ldb,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8771-8796 / lapack/roclapack_getrs_strided_batched.cpp:74-108 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrs_strided_batched(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    float* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8872-8890 / lapack/roclapack_gesv.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgesv(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    float* B,
+    const rocblas_int ldb,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:8970-8992 / lapack/roclapack_gesv_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgesv_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    float* const B[],
+    const rocblas_int ldb,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9095-9108 / lapack/roclapack_gesv_strided_batched.cpp:92-127 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgesv_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    float* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10188-10201 / lapack/roclapack_potrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_spotrf(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:10261-10276 / lapack/roclapack_potrf_batched.cpp:86 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_spotrf_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    float* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10340-10356 / lapack/roclapack_potrf_strided_batched.cpp:84-110 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_spotrf_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10426-10443 / lapack/roclapack_potrs.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_spotrs(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    float* B,
+    const rocblas_int ldb);
+
+/* replaces rocsolver-functions.h:10520-10538 / lapack/roclapack_potrs_batched.cpp:72 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_spotrs_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* const A[],
+    const rocblas_int lda,
+    float* const B[],
+    const rocblas_int ldb,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10619-10642 / lapack/roclapack_potrs_strided_batched.cpp:71-102 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_spotrs_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    float* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10718-10736 / lapack/roclapack_posv.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sposv(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    float* B,
+    const rocblas_int ldb,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:10816-10833 / lapack/roclapack_posv_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sposv_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* const A[],
+    const rocblas_int lda,
+    float* const B[],
+    const rocblas_int ldb,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10931-10944 / lapack/roclapack_posv_strided_batched.cpp:87 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sposv_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    float* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:5139-5155 / lapack/roclapack_getrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrf(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:5227-5247 / lapack/roclapack_getrf_batched.cpp:96-124 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrf_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    double* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:5329-5349 / lapack/roclapack_getrf_strided_batched.cpp:94-122 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrf_strided_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:4609-4622 / lapack/roclapack_getrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrf_npvt(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:4688-4702 / lapack/roclapack_getrf_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrf_npvt_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    double* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:4775-4790 / lapack/roclapack_getrf_strided_batched.cpp:154-208 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrf_npvt_strided_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8562-8580 / lapack/roclapack_getrs.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrs(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_int* ipiv,
+    double* B,
+    const rocblas_int ldb);
+
+/* replaces rocsolver-functions.h:8657-8680 / lapack/roclapack_getrs_batched.cpp:75 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrs_batched(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* const A[],
+    const rocblas_int lda,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    double* const B[],
+    const rocblas_int ldb,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8771-8796 / lapack/roclapack_getrs_strided_batched.cpp:74-108 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrs_strided_batched(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    double* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8872-8890 / lapack/roclapack_gesv.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    double* B,
+    const rocblas_int ldb,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:8970-8992 / lapack/roclapack_gesv_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    double* const B[],
+    const rocblas_int ldb,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9095-9108 / lapack/roclapack_gesv_strided_batched.cpp:92-127 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    double* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10188-10201 / lapack/roclapack_potrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dpotrf(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:10261-10276 / lapack/roclapack_potrf_batched.cpp:86 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dpotrf_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    double* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10340-10356 / lapack/roclapack_potrf_strided_batched.cpp:84-110 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dpotrf_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10426-10443 / lapack/roclapack_potrs.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dpotrs(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    double* B,
+    const rocblas_int ldb);
+
+/* replaces rocsolver-functions.h:10520-10538 / lapack/roclapack_potrs_batched.cpp:72 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dpotrs_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* const A[],
+    const rocblas_int lda,
+    double* const B[],
+    const rocblas_int ldb,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10619-10642 / lapack/roclapack_potrs_strided_batched.cpp:71-102 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dpotrs_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    double* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10718-10736 / lapack/roclapack_posv.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dposv(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    double* B,
+    const rocblas_int ldb,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:10816-10833 / lapack/roclapack_posv_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dposv_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* const A[],
+    const rocblas_int lda,
+    double* const B[],
+    const rocblas_int ldb,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10931-10944 / lapack/roclapack_posv_strided_batched.cpp:87 */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dposv_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    double* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ROCSOLVER_B200_ROCSOLVER_H */

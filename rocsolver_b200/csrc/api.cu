@@ -1,0 +1,331 @@
+// api.cpp -- extern "C" entry points with the reference's names, argument order and
+// argument-check order.  Each *_impl restates the reference's _impl + argCheck pair:
+//   getrf : lapack/roclapack_getrf_strided_batched.cpp:8-84, roclapack_getf2.hpp:489-517
+//   getrs : lapack/roclapack_getrs_strided_batched.cpp:8-72, roclapack_getrs.hpp:17-49
+//   gesv  : lapack/roclapack_gesv_strided_batched.cpp:8-90, roclapack_gesv.hpp:18-47,105-178
+//   potrf : lapack/roclapack_potrf_strided_batched.cpp:8-82, roclapack_potf2.hpp:107-134
+//   potrs : lapack/roclapack_potrs_strided_batched.cpp:8-70, roclapack_potrs.hpp:17-46
+//   posv  : lapack/roclapack_posv_strided_batched.cpp, roclapack_posv.hpp:18-47,101-170
+// Order of checks: invalid_handle, invalid_value (enum arguments), invalid_size, then a
+// device-memory size query returns here, then invalid_pointer, then quick returns.
+#include "handle.h"
+#include "launch.h"
+
+using namespace rsb;
+
+namespace {
+
+inline bool bad_op(rocblas_operation t)
+{
+    return t != rocblas_operation_none && t != rocblas_operation_transpose
+           && t != rocblas_operation_conjugate_transpose;
+}
+inline bool bad_fill(rocblas_fill f)
+{
+    return f != rocblas_fill_upper && f != rocblas_fill_lower;
+}
+
+template <typename T>
+rocblas_status getrf_impl(rocblas_handle h, int m, int n, Batch<T> A, const void* Aptr, int lda,
+                          int* ipiv, int64_t strideP, int* info, int bc, bool pivot)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(m < 0 || n < 0 || lda < m || bc < 0)
+        return rocblas_status_invalid_size;
+    if(h->querying)
+        return ws_query(h, 0);
+    const int64_t mn = (int64_t)m * n;
+    if((mn && !Aptr) || (mn && pivot && !ipiv) || (bc && !info))
+        return rocblas_status_invalid_pointer;
+    if(bc == 0)
+        return rocblas_status_success;
+    if(m == 0 || n == 0)
+        return launch_reset_info(h->stream, info, bc);
+    return launch_getrf<T>(h->stream, m, n, A, lda, ipiv, strideP, info, bc, pivot);
+}
+
+template <typename T>
+rocblas_status getrs_impl(rocblas_handle h, rocblas_operation trans, int n, int nrhs,
+                          Batch<T> A, const void* Aptr, int lda, const int* ipiv,
+                          int64_t strideP, Batch<T> B, const void* Bptr, int ldb, int bc)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(bad_op(trans))
+        return rocblas_status_invalid_value;
+    if(n < 0 || nrhs < 0 || lda < n || ldb < n || bc < 0)
+        return rocblas_status_invalid_size;
+    if(h->querying)
+        return ws_query(h, 0);
+    if((n && !Aptr) || (n && !ipiv) || ((int64_t)nrhs * n && !Bptr))
+        return rocblas_status_invalid_pointer;
+    if(n == 0 || nrhs == 0 || bc == 0)
+        return rocblas_status_success;
+    return launch_getrs<T>(h->stream, trans == rocblas_operation_none ? 0 : 1, n, nrhs, A, lda,
+                           ipiv, strideP, B, ldb, nullptr, bc);
+}
+
+template <typename T>
+rocblas_status gesv_impl(rocblas_handle h, int n, int nrhs, Batch<T> A, const void* Aptr,
+                         int lda, int* ipiv, int64_t strideP, Batch<T> B, const void* Bptr,
+                         int ldb, int* info, int bc)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(n < 0 || nrhs < 0 || lda < n || ldb < n || bc < 0)
+        return rocblas_status_invalid_size;
+    if(h->querying)
+        return ws_query(h, 0);
+    if((n && !Aptr) || (n && !ipiv) || ((int64_t)nrhs * n && !Bptr) || (bc && !info))
+        return rocblas_status_invalid_pointer;
+    if(bc == 0)
+        return rocblas_status_success;
+    // the reference zeroes info and returns without factoring when A or B is empty
+    if(n == 0 || nrhs == 0)
+        return launch_reset_info(h->stream, info, bc);
+    return launch_gesv<T>(h->stream, n, nrhs, A, lda, ipiv, strideP, B, ldb, info, bc);
+}
+
+template <typename T>
+rocblas_status potrf_impl(rocblas_handle h, rocblas_fill uplo, int n, Batch<T> A,
+                          const void* Aptr, int lda, int* info, int bc)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(bad_fill(uplo))
+        return rocblas_status_invalid_value;
+    if(n < 0 || lda < n || bc < 0)
+        return rocblas_status_invalid_size;
+    if(h->querying)
+        return ws_query(h, 0);
+    if((n && !Aptr) || (bc && !info))
+        return rocblas_status_invalid_pointer;
+    if(bc == 0)
+        return rocblas_status_success;
+    if(n == 0)
+        return launch_reset_info(h->stream, info, bc);
+    return launch_potrf<T>(h->stream, uplo == rocblas_fill_upper, n, A, lda, info, bc);
+}
+
+template <typename T>
+rocblas_status potrs_impl(rocblas_handle h, rocblas_fill uplo, int n, int nrhs, Batch<T> A,
+                          const void* Aptr, int lda, Batch<T> B, const void* Bptr, int ldb,
+                          int bc)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(bad_fill(uplo))
+        return rocblas_status_invalid_value;
+    if(n < 0 || nrhs < 0 || lda < n || ldb < n || bc < 0)
+        return rocblas_status_invalid_size;
+    if(h->querying)
+        return ws_query(h, 0);
+    if((n && !Aptr) || ((int64_t)nrhs * n && !Bptr))
+        return rocblas_status_invalid_pointer;
+    if(n == 0 || nrhs == 0 || bc == 0)
+        return rocblas_status_success;
+    return launch_potrs<T>(h->stream, uplo == rocblas_fill_upper, n, nrhs, A, lda, B, ldb,
+                           nullptr, bc);
+}
+
+template <typename T>
+rocblas_status posv_impl(rocblas_handle h, rocblas_fill uplo, int n, int nrhs, Batch<T> A,
+                         const void* Aptr, int lda, Batch<T> B, const void* Bptr, int ldb,
+                         int* info, int bc)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(bad_fill(uplo))
+        return rocblas_status_invalid_value;
+    if(n < 0 || nrhs < 0 || lda < n || ldb < n || bc < 0)
+        return rocblas_status_invalid_size;
+    if(h->querying)
+        return ws_query(h, 0);
+    if((n && !Aptr) || ((int64_t)nrhs * n && !Bptr) || (bc && !info))
+        return rocblas_status_invalid_pointer;
+    if(bc == 0)
+        return rocblas_status_success;
+    if(n == 0 || nrhs == 0)
+        return launch_reset_info(h->stream, info, bc);
+    const int up = uplo == rocblas_fill_upper;
+    rocblas_status st = launch_potrf<T>(h->stream, up, n, A, lda, info, bc);
+    if(st != rocblas_status_success)
+        return st;
+    return launch_potrs<T>(h->stream, up, n, nrhs, A, lda, B, ldb, info, bc);
+}
+
+} // namespace
+
+#define RSB_API_TYPE(P, T)                                                                      \
+    rocblas_status rocsolver_##P##getrf(rocblas_handle handle, const rocblas_int m,             \
+                                        const rocblas_int n, T* A, const rocblas_int lda,      \
+                                        rocblas_int* ipiv, rocblas_int* info)                  \
+    {                                                                                           \
+        return getrf_impl<T>(handle, m, n, strided<T>(A, 0), A, lda, ipiv, 0, info, 1, true);   \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrf_batched(rocblas_handle handle, const rocblas_int m,     \
+                                                const rocblas_int n, T* const A[],              \
+                                                const rocblas_int lda, rocblas_int* ipiv,       \
+                                                const rocblas_stride strideP, rocblas_int* info,\
+                                                const rocblas_int batch_count)                  \
+    {                                                                                           \
+        return getrf_impl<T>(handle, m, n, pointers<T>(A), A, lda, ipiv, strideP, info,         \
+                             batch_count, true);                                                \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrf_strided_batched(                                        \
+        rocblas_handle handle, const rocblas_int m, const rocblas_int n, T* A,                 \
+        const rocblas_int lda, const rocblas_stride strideA, rocblas_int* ipiv,                \
+        const rocblas_stride strideP, rocblas_int* info, const rocblas_int batch_count)        \
+    {                                                                                           \
+        return getrf_impl<T>(handle, m, n, strided<T>(A, strideA), A, lda, ipiv, strideP,      \
+                             info, batch_count, true);                                          \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrf_npvt(rocblas_handle handle, const rocblas_int m,        \
+                                             const rocblas_int n, T* A, const rocblas_int lda, \
+                                             rocblas_int* info)                                 \
+    {                                                                                           \
+        return getrf_impl<T>(handle, m, n, strided<T>(A, 0), A, lda, nullptr, 0, info, 1,      \
+                             false);                                                            \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrf_npvt_batched(                                           \
+        rocblas_handle handle, const rocblas_int m, const rocblas_int n, T* const A[],         \
+        const rocblas_int lda, rocblas_int* info, const rocblas_int batch_count)               \
+    {                                                                                           \
+        return getrf_impl<T>(handle, m, n, pointers<T>(A), A, lda, nullptr, 0, info,            \
+                             batch_count, false);                                               \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrf_npvt_strided_batched(                                   \
+        rocblas_handle handle, const rocblas_int m, const rocblas_int n, T* A,                 \
+        const rocblas_int lda, const rocblas_stride strideA, rocblas_int* info,                \
+        const rocblas_int batch_count)                                                          \
+    {                                                                                           \
+        return getrf_impl<T>(handle, m, n, strided<T>(A, strideA), A, lda, nullptr, 0, info,   \
+                             batch_count, false);                                               \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrs(rocblas_handle handle, const rocblas_operation trans,   \
+                                        const rocblas_int n, const rocblas_int nrhs, T* A,     \
+                                        const rocblas_int lda, const rocblas_int* ipiv, T* B,  \
+                                        const rocblas_int ldb)                                  \
+    {                                                                                           \
+        return getrs_impl<T>(handle, trans, n, nrhs, strided<T>(A, 0), A, lda, ipiv, 0,         \
+                             strided<T>(B, 0), B, ldb, 1);                                      \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrs_batched(                                                \
+        rocblas_handle handle, const rocblas_operation trans, const rocblas_int n,             \
+        const rocblas_int nrhs, T* const A[], const rocblas_int lda, const rocblas_int* ipiv,  \
+        const rocblas_stride strideP, T* const B[], const rocblas_int ldb,                     \
+        const rocblas_int batch_count)                                                          \
+    {                                                                                           \
+        return getrs_impl<T>(handle, trans, n, nrhs, pointers<T>(A), A, lda, ipiv, strideP,     \
+                             pointers<T>(B), B, ldb, batch_count);                              \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrs_strided_batched(                                        \
+        rocblas_handle handle, const rocblas_operation trans, const rocblas_int n,             \
+        const rocblas_int nrhs, T* A, const rocblas_int lda, const rocblas_stride strideA,     \
+        const rocblas_int* ipiv, const rocblas_stride strideP, T* B, const rocblas_int ldb,    \
+        const rocblas_stride strideB, const rocblas_int batch_count)                           \
+    {                                                                                           \
+        return getrs_impl<T>(handle, trans, n, nrhs, strided<T>(A, strideA), A, lda, ipiv,      \
+                             strideP, strided<T>(B, strideB), B, ldb, batch_count);             \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##gesv(rocblas_handle handle, const rocblas_int n,              \
+                                       const rocblas_int nrhs, T* A, const rocblas_int lda,    \
+                                       rocblas_int* ipiv, T* B, const rocblas_int ldb,         \
+                                       rocblas_int* info)                                      \
+    {                                                                                           \
+        return gesv_impl<T>(handle, n, nrhs, strided<T>(A, 0), A, lda, ipiv, 0,                 \
+                            strided<T>(B, 0), B, ldb, info, 1);                                 \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##gesv_batched(                                                 \
+        rocblas_handle handle, const rocblas_int n, const rocblas_int nrhs, T* const A[],      \
+        const rocblas_int lda, rocblas_int* ipiv, const rocblas_stride strideP, T* const B[],  \
+        const rocblas_int ldb, rocblas_int* info, const rocblas_int batch_count)               \
+    {                                                                                           \
+        return gesv_impl<T>(handle, n, nrhs, pointers<T>(A), A, lda, ipiv, strideP,             \
+                            pointers<T>(B), B, ldb, info, batch_count);                         \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##gesv_strided_batched(                                         \
+        rocblas_handle handle, const rocblas_int n, const rocblas_int nrhs, T* A,              \
+        const rocblas_int lda, const rocblas_stride strideA, rocblas_int* ipiv,                \
+        const rocblas_stride strideP, T* B, const rocblas_int ldb,                             \
+        const rocblas_stride strideB, rocblas_int* info, const rocblas_int batch_count)        \
+    {                                                                                           \
+        return gesv_impl<T>(handle, n, nrhs, strided<T>(A, strideA), A, lda, ipiv, strideP,     \
+                            strided<T>(B, strideB), B, ldb, info, batch_count);                 \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##potrf(rocblas_handle handle, const rocblas_fill uplo,         \
+                                        const rocblas_int n, T* A, const rocblas_int lda,      \
+                                        rocblas_int* info)                                      \
+    {                                                                                           \
+        return potrf_impl<T>(handle, uplo, n, strided<T>(A, 0), A, lda, info, 1);               \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##potrf_batched(rocblas_handle handle, const rocblas_fill uplo, \
+                                                const rocblas_int n, T* const A[],              \
+                                                const rocblas_int lda, rocblas_int* info,       \
+                                                const rocblas_int batch_count)                  \
+    {                                                                                           \
+        return potrf_impl<T>(handle, uplo, n, pointers<T>(A), A, lda, info, batch_count);       \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##potrf_strided_batched(                                        \
+        rocblas_handle handle, const rocblas_fill uplo, const rocblas_int n, T* A,             \
+        const rocblas_int lda, const rocblas_stride strideA, rocblas_int* info,                \
+        const rocblas_int batch_count)                                                          \
+    {                                                                                           \
+        return potrf_impl<T>(handle, uplo, n, strided<T>(A, strideA), A, lda, info,             \
+                             batch_count);                                                      \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##potrs(rocblas_handle handle, const rocblas_fill uplo,         \
+                                        const rocblas_int n, const rocblas_int nrhs, T* A,     \
+                                        const rocblas_int lda, T* B, const rocblas_int ldb)    \
+    {                                                                                           \
+        return potrs_impl<T>(handle, uplo, n, nrhs, strided<T>(A, 0), A, lda,                   \
+                             strided<T>(B, 0), B, ldb, 1);                                      \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##potrs_batched(                                                \
+        rocblas_handle handle, const rocblas_fill uplo, const rocblas_int n,                   \
+        const rocblas_int nrhs, T* const A[], const rocblas_int lda, T* const B[],             \
+        const rocblas_int ldb, const rocblas_int batch_count)                                  \
+    {                                                                                           \
+        return potrs_impl<T>(handle, uplo, n, nrhs, pointers<T>(A), A, lda, pointers<T>(B), B,  \
+                             ldb, batch_count);                                                 \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##potrs_strided_batched(                                        \
+        rocblas_handle handle, const rocblas_fill uplo, const rocblas_int n,                   \
+        const rocblas_int nrhs, T* A, const rocblas_int lda, const rocblas_stride strideA,     \
+        T* B, const rocblas_int ldb, const rocblas_stride strideB,                             \
+        const rocblas_int batch_count)                                                          \
+    {                                                                                           \
+        return potrs_impl<T>(handle, uplo, n, nrhs, strided<T>(A, strideA), A, lda,             \
+                             strided<T>(B, strideB), B, ldb, batch_count);                      \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##posv(rocblas_handle handle, const rocblas_fill uplo,          \
+                                       const rocblas_int n, const rocblas_int nrhs, T* A,      \
+                                       const rocblas_int lda, T* B, const rocblas_int ldb,     \
+                                       rocblas_int* info)                                      \
+    {                                                                                           \
+        return posv_impl<T>(handle, uplo, n, nrhs, strided<T>(A, 0), A, lda, strided<T>(B, 0),  \
+                            B, ldb, info, 1);                                                   \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##posv_batched(                                                 \
+        rocblas_handle handle, const rocblas_fill uplo, const rocblas_int n,                   \
+        const rocblas_int nrhs, T* const A[], const rocblas_int lda, T* const B[],             \
+        const rocblas_int ldb, rocblas_int* info, const rocblas_int batch_count)               \
+    {                                                                                           \
+        return posv_impl<T>(handle, uplo, n, nrhs, pointers<T>(A), A, lda, pointers<T>(B), B,   \
+                            ldb, info, batch_count);                                            \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##posv_strided_batched(                                         \
+        rocblas_handle handle, const rocblas_fill uplo, const rocblas_int n,                   \
+        const rocblas_int nrhs, T* A, const rocblas_int lda, const rocblas_stride strideA,     \
+        T* B, const rocblas_int ldb, const rocblas_stride strideB, rocblas_int* info,          \
+        const rocblas_int batch_count)                                                          \
+    {                                                                                           \
+        return posv_impl<T>(handle, uplo, n, nrhs, strided<T>(A, strideA), A, lda,              \
+                            strided<T>(B, strideB), B, ldb, info, batch_count);                 \
+    }
+
+extern "C" {
+RSB_API_TYPE(s, float)
+RSB_API_TYPE(d, double)
+}

@@ -1,0 +1,183 @@
+// chol.cuh -- CTA-per-matrix blocked Cholesky for general n (lower or upper).
+//
+// Replaces the reference's potrf (library/src/lapack/roclapack_potrf.hpp:90-228) and its
+// unblocked potf2 (library/src/lapack/roclapack_potf2.hpp:137-253), which at n = 64 issues
+// ~256 launches per call (dot, sqrtDiagOnward with 1-thread blocks, gemv, scal per column).
+//
+// B200 design: ONE launch, one CTA per matrix.  The panel (rows j0..n-1 of JB columns of
+// the referenced triangle) is held in registers, one or more rows per thread.  Per column
+// the rows of the diagonal block publish their current column value to shared memory and
+// one barrier later every thread has the pivot and the column of L it needs for its own
+// rank-1 update.  For n <= JB (e.g. n = 64) the whole factorisation is one panel.  Wider
+// matrices apply the panel to the trailing triangle (SYRK) with the L21 rows still in
+// registers and the transposed operand broadcast from shared memory.
+//
+// The upper case (A = U' U) is the lower algorithm on the transposed view
+// M(r, c) = A[c + r*lda].  The first non-positive (or NaN) pivot is stored, info is set to
+// its 1-based index and the factorisation stops, as LAPACK dpotf2 does; the reference
+// (sqrtDiagOnward, :16-43) records the same info.
+#pragma once
+
+#include "common.cuh"
+
+namespace rsb {
+
+template <typename T, int NT, int R, int JB>
+struct CtaCholSmem
+{
+    static __host__ __device__ size_t bytes(int n)
+    {
+        (void)n;
+        size_t s = sizeof(T) * 2 * JB + sizeof(T) * (size_t)R * NT * (JB + 1);
+        return (s + 15) & ~size_t(15);
+    }
+};
+
+template <typename T, int NT, int R, int JB, int TN>
+__global__ void __launch_bounds__(NT)
+    potrf_cta_kernel(int upper, int n, Batch<T> A, int lda, int* info)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* scol = reinterpret_cast<T*>(smem_raw);      // [2][JB]
+    T* sL = scol + 2 * JB;                           // [R*NT][JB+1] trailing L rows
+    constexpr int LDL = JB + 1;
+    const int tid = threadIdx.x;
+    const int64_t b = blockIdx.x;
+    T* a = A.at(b);
+    const int64_t rs = upper ? lda : 1, cs = upper ? 1 : lda;
+    auto at = [&](int r, int c) -> T& { return a[(int64_t)r * rs + (int64_t)c * cs]; };
+
+    T pv[R][JB];
+    int inf = 0;
+    for(int j0 = 0; j0 < n && inf == 0; j0 += JB)
+    {
+        const int jb = min(JB, n - j0);
+        const int mp = n - j0;
+#pragma unroll
+        for(int q = 0; q < R; ++q)
+        {
+            const int r = tid + q * NT;
+#pragma unroll
+            for(int c = 0; c < JB; ++c)
+                pv[q][c] = (r < mp && c < jb && c <= r) ? at(j0 + r, j0 + c) : T(0);
+        }
+        int cfail = JB;
+#pragma unroll
+        for(int c = 0; c < JB; ++c)
+        {
+            if(c < jb && cfail == JB)
+            {
+                const int buf = c & 1;
+                T* sc = scol + buf * JB;
+#pragma unroll
+                for(int q = 0; q < R; ++q)
+                {
+                    const int r = tid + q * NT;
+                    if(r >= c && r < jb)
+                        sc[r] = pv[q][c];
+                }
+                __syncthreads();
+                const T d = sc[c];
+                if(!(d > T(0)))
+                {
+                    cfail = c; // uniform: every thread read the same d
+                    break;
+                }
+                const T s = sqrt(d);
+                const T rcp = T(1) / s;
+#pragma unroll
+                for(int q = 0; q < R; ++q)
+                {
+                    const int r = tid + q * NT;
+                    if(r == c)
+                        pv[q][c] = s;
+                    else if(r > c && r < mp)
+                    {
+                        const T l = pv[q][c] * rcp;
+                        pv[q][c] = l;
+#pragma unroll
+                        for(int cc = 0; cc < JB; ++cc)
+                            if(cc > c && cc < jb && cc <= r)
+                                pv[q][cc] = fma(-l, sc[cc] * rcp, pv[q][cc]);
+                    }
+                }
+            }
+        }
+        // write back the factored columns (all of them on success; up to the failing
+        // one otherwise, whose non-positive value is stored as LAPACK does)
+        const int cdone = cfail == JB ? jb : cfail;
+#pragma unroll
+        for(int q = 0; q < R; ++q)
+        {
+            const int r = tid + q * NT;
+            if(r < mp)
+            {
+#pragma unroll
+                for(int c = 0; c < JB; ++c)
+                    if(c < jb && c <= r && (c < cdone || (c == cdone && r == cdone)))
+                        at(j0 + r, j0 + c) = pv[q][c];
+                if(r >= jb && cfail == JB)
+                {
+#pragma unroll
+                    for(int c = 0; c < JB; ++c)
+                        sL[(size_t)(r - jb) * LDL + c] = pv[q][c];
+                }
+            }
+        }
+        if(cfail != JB)
+        {
+            inf = j0 + cfail + 1;
+            break;
+        }
+        __syncthreads();
+        // trailing update A22 -= L21 L21' (lower triangle only)
+        const int nt = mp - jb;
+        for(int t0 = 0; t0 < nt; t0 += TN)
+        {
+            T acc[R][TN];
+#pragma unroll
+            for(int q = 0; q < R; ++q)
+            {
+                const int rt = tid + q * NT - jb;
+#pragma unroll
+                for(int t = 0; t < TN; ++t)
+                    acc[q][t] = (rt >= 0 && rt < nt && t0 + t <= rt)
+                                    ? at(j0 + jb + rt, j0 + jb + t0 + t)
+                                    : T(0);
+            }
+#pragma unroll
+            for(int k = 0; k < JB; ++k)
+            {
+                if(k < jb)
+                {
+                    T lk[TN];
+#pragma unroll
+                    for(int t = 0; t < TN; ++t)
+                        lk[t] = t0 + t < nt ? sL[(size_t)(t0 + t) * LDL + k] : T(0);
+#pragma unroll
+                    for(int q = 0; q < R; ++q)
+#pragma unroll
+                        for(int t = 0; t < TN; ++t)
+                            acc[q][t] = fma(-pv[q][k], lk[t], acc[q][t]);
+                }
+            }
+#pragma unroll
+            for(int q = 0; q < R; ++q)
+            {
+                const int rt = tid + q * NT - jb;
+                if(rt >= 0 && rt < nt)
+                {
+#pragma unroll
+                    for(int t = 0; t < TN; ++t)
+                        if(t0 + t <= rt)
+                            at(j0 + jb + rt, j0 + jb + t0 + t) = acc[q][t];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if(tid == 0)
+        info[b] = inf;
+}
+
+} // namespace rsb

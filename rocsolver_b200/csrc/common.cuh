@@ -1,0 +1,155 @@
+// common.cuh -- device helpers shared by the LU and Cholesky kernels.
+//
+// Layout conventions are the reference's (library/src/include/lib_host_helpers.hpp:21-24
+// idx2D = i + j*lda; common/include/rocblas_utility.hpp:97-118 load_ptr_batch): member b of
+// a strided batch starts at A + b*strideA, member b of a pointer-array batch is A[b].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <float.h>
+#include <limits.h>
+
+namespace rsb {
+
+// ---------------------------------------------------------------------------------------
+// batch addressing: strided (ptrs == nullptr) or pointer array (ptrs != nullptr)
+template <typename T>
+struct Batch
+{
+    T* base;
+    T* const* ptrs;
+    int64_t stride;
+    __device__ __forceinline__ T* at(int64_t b) const
+    {
+        return ptrs ? ptrs[b] : base + b * stride;
+    }
+};
+
+template <typename T>
+__host__ __device__ inline Batch<T> strided(T* p, int64_t s)
+{
+    return Batch<T>{p, nullptr, s};
+}
+template <typename T>
+__host__ __device__ inline Batch<T> pointers(T* const* p)
+{
+    return Batch<T>{nullptr, p, 0};
+}
+
+__device__ __forceinline__ size_t ix(int i, int j, int ld)
+{
+    return (size_t)i + (size_t)j * (size_t)ld;
+}
+
+template <typename T>
+struct Lim;
+template <>
+struct Lim<double>
+{
+    static __device__ __forceinline__ double sfmin() { return DBL_MIN; }
+};
+template <>
+struct Lim<float>
+{
+    static __device__ __forceinline__ float sfmin() { return FLT_MIN; }
+};
+
+// ---------------------------------------------------------------------------------------
+// Pivot keys.  LAPACK's idamax (and the reference's iamax,
+// library/src/include/lapack_device_functions.hpp:680-740) returns the FIRST index of
+// the largest |x|, scanning with a strict '>' so that a NaN never replaces the running
+// maximum.  A tree reduction reproduces that sequential rule exactly when:
+//   key(x) = bit pattern of |x| (monotone in |x| for non-negative IEEE values),
+//   a NaN in the first candidate row (row k) gets the largest key (it can never be
+//   replaced), a NaN elsewhere gets key 0 (it can never win against row k), and
+//   ties on the key go to the smallest logical row index.
+__device__ __forceinline__ uint64_t pivot_key(double x, bool first_row)
+{
+    uint64_t u = (uint64_t)__double_as_longlong(x) & 0x7fffffffffffffffull;
+    if(u > 0x7ff0000000000000ull)
+        u = first_row ? 0xffffffffffffffffull : 0ull;
+    return u;
+}
+__device__ __forceinline__ uint32_t pivot_key(float x, bool first_row)
+{
+    uint32_t u = (uint32_t)__float_as_uint(x) & 0x7fffffffu;
+    if(u > 0x7f800000u)
+        u = first_row ? 0xffffffffu : 0u;
+    return u;
+}
+
+template <typename T>
+struct KeyOf;
+template <>
+struct KeyOf<double>
+{
+    using type = uint64_t;
+};
+template <>
+struct KeyOf<float>
+{
+    using type = uint32_t;
+};
+
+// Warp-wide argmax over (key, row) pairs: largest key, then smallest row.  Lanes with
+// valid == false do not take part.  Returns the winning row (INT_MAX if none is valid)
+// and the winning key through *kout.  Uses redux.sync (3 for 64-bit keys, 2 for 32-bit).
+__device__ __forceinline__ int warp_argmax(uint64_t key, int row, bool valid, uint64_t* kout)
+{
+    const unsigned full = 0xffffffffu;
+    uint32_t hi = valid ? (uint32_t)(key >> 32) : 0u;
+    uint32_t mhi = __reduce_max_sync(full, hi);
+    uint32_t lo = (valid && hi == mhi) ? (uint32_t)key : 0u;
+    uint32_t mlo = __reduce_max_sync(full, lo);
+    bool match = valid && hi == mhi && (uint32_t)key == mlo;
+    int r = (int)__reduce_min_sync(full, (unsigned)(match ? row : INT_MAX));
+    *kout = ((uint64_t)mhi << 32) | mlo;
+    return r;
+}
+__device__ __forceinline__ int warp_argmax(uint32_t key, int row, bool valid, uint32_t* kout)
+{
+    const unsigned full = 0xffffffffu;
+    uint32_t k = valid ? key : 0u;
+    uint32_t mk = __reduce_max_sync(full, k);
+    bool match = valid && key == mk;
+    int r = (int)__reduce_min_sync(full, (unsigned)(match ? row : INT_MAX));
+    *kout = mk;
+    return r;
+}
+
+// LAPACK getf2 column scaling: multiply by the reciprocal when |pivot| >= sfmin,
+// otherwise divide (dgetf2; the reference always multiplies,
+// specialized/roclapack_getf2_specialized_kernels.hpp:96-99, which differs only for
+// subnormal pivots).  A zero pivot leaves the column unscaled.
+template <typename T>
+struct Scaler
+{
+    T piv, rcp;
+    int mode; // 0: zero pivot (no scaling), 1: multiply by rcp, 2: divide by piv
+    __device__ __forceinline__ void init(T p)
+    {
+        piv = p;
+        if(p == T(0))
+        {
+            mode = 0;
+            rcp = T(0);
+        }
+        else if(fabs(p) >= Lim<T>::sfmin())
+        {
+            mode = 1;
+            rcp = T(1) / p;
+        }
+        else
+        {
+            mode = 2;
+            rcp = T(0);
+        }
+    }
+    __device__ __forceinline__ T apply(T x) const
+    {
+        return mode == 1 ? x * rcp : (mode == 2 ? x / piv : x);
+    }
+};
+
+} // namespace rsb

@@ -1,0 +1,274 @@
+// lu.cu -- launchers for getrf / getrs / gesv and the Cholesky pair.
+//
+// Kernel selection by size replaces the reference's compile-time tuning tables
+// (library/src/include/ideal_sizes.hpp:208-240 getrf, :166-180 potrf;
+// roclapack_getf2.hpp:181-276 select_spkernel).
+#include "chol.cuh"
+#include "launch.h"
+#include "lu_cta.cuh"
+#include "lu_small.cuh"
+#include "trsv.cuh"
+
+namespace rsb {
+
+static inline rocblas_status launch_status()
+{
+    return cudaGetLastError() == cudaSuccess ? rocblas_status_success
+                                             : rocblas_status_internal_error;
+}
+
+template <typename K>
+static inline bool set_smem(K kernel, size_t bytes)
+{
+    if(bytes <= 48 * 1024)
+        return true;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bytes)
+           == cudaSuccess;
+}
+
+__global__ void reset_info_kernel(int* info, int bc)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < bc)
+        info[i] = 0;
+}
+
+rocblas_status launch_reset_info(cudaStream_t s, int* info, int bc)
+{
+    if(bc <= 0)
+        return rocblas_status_success;
+    reset_info_kernel<<<(bc + 255) / 256, 256, 0, s>>>(info, bc);
+    return launch_status();
+}
+
+// ------------------------------------------------------------------------------ getrf
+template <typename T, int NMAX, bool PIVOT>
+static void run_getrf_warp(cudaStream_t s, int m, int n, Batch<T> A, int lda, int* ipiv,
+                           int64_t sP, int* info, int bc)
+{
+    dim3 grid((bc + SMALL_WPB - 1) / SMALL_WPB);
+    getrf_warp_kernel<T, NMAX, PIVOT><<<grid, 32 * SMALL_WPB, 0, s>>>(m, n, A, lda, ipiv, sP,
+                                                                       info, bc);
+}
+
+template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
+static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, int lda,
+                                    int* ipiv, int64_t sP, int* info, int bc)
+{
+    // U12 chunk width: multiple of TN, at most 64 KiB of shared memory
+    int cw = (int)((64 * 1024) / (sizeof(T) * JB));
+    cw = cw / TN * TN;
+    const int need = ((n + TN - 1) / TN) * TN;
+    if(need < cw)
+        cw = need < TN ? TN : need;
+    const size_t smem = CtaLuSmem<T, NT, JB>::bytes(cw, R);
+    auto k = getrf_cta_kernel<T, NT, R, JB, TN, PIVOT>;
+    if(!set_smem(k, smem))
+        return rocblas_status_internal_error;
+    k<<<bc, NT, smem, s>>>(m, n, A, lda, ipiv, sP, info, cw);
+    return launch_status();
+}
+
+template <typename T, bool PIVOT>
+static rocblas_status getrf_dispatch(cudaStream_t s, int m, int n, Batch<T> A, int lda,
+                                     int* ipiv, int64_t sP, int* info, int bc)
+{
+    if(m <= 32 && n <= 32)
+    {
+        if(n <= 8)
+            run_getrf_warp<T, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+        else if(n <= 16)
+            run_getrf_warp<T, 16, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+        else
+            run_getrf_warp<T, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+        return launch_status();
+    }
+    if(m <= 64)
+        return run_getrf_cta<T, 64, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+    if(m <= 128)
+        return run_getrf_cta<T, 128, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+    if(m <= 256)
+        return run_getrf_cta<T, 256, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+    if(m <= 512)
+        return run_getrf_cta<T, 256, 2, 16, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+    if(m <= 1024)
+        return run_getrf_cta<T, 256, 4, 8, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+    if(m <= MAX_CTA_ROWS)
+        return run_getrf_cta<T, 256, 8, 4, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+    return rocblas_status_not_implemented;
+}
+
+template <typename T>
+rocblas_status launch_getrf(cudaStream_t s, int m, int n, Batch<T> A, int lda, int* ipiv,
+                            int64_t sP, int* info, int bc, bool pivot)
+{
+    return pivot ? getrf_dispatch<T, true>(s, m, n, A, lda, ipiv, sP, info, bc)
+                 : getrf_dispatch<T, false>(s, m, n, A, lda, ipiv, sP, info, bc);
+}
+
+// ------------------------------------------------------------------------------ getrs
+template <typename T, int NMAX, int NRC>
+static void run_getrs_warp(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A, int lda,
+                           const int* ipiv, int64_t sP, Batch<T> B, int ldb, const int* skip,
+                           int bc)
+{
+    const int64_t tasks = (int64_t)bc * ((nrhs + NRC - 1) / NRC);
+    dim3 grid((unsigned)((tasks + SMALL_WPB - 1) / SMALL_WPB));
+    getrs_warp_kernel<T, NMAX, NRC><<<grid, 32 * SMALL_WPB, 0, s>>>(trans, n, nrhs, A, lda, ipiv,
+                                                                     sP, B, ldb, skip, bc);
+}
+
+template <typename T, int NMAX>
+static void getrs_warp_nrc(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A, int lda,
+                           const int* ipiv, int64_t sP, Batch<T> B, int ldb, const int* skip,
+                           int bc)
+{
+    if(nrhs == 1)
+        run_getrs_warp<T, NMAX, 1>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+    else
+        run_getrs_warp<T, NMAX, 4>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+}
+
+template <typename T, int NRC>
+static rocblas_status run_getrs_cta(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A,
+                                    int lda, const int* ipiv, int64_t sP, Batch<T> B, int ldb,
+                                    const int* skip, int bc)
+{
+    const size_t smem = sizeof(T) * (size_t)n * NRC + sizeof(int) * (size_t)n;
+    auto k = getrs_cta_kernel<T, 256, NRC>;
+    if(!set_smem(k, smem))
+        return rocblas_status_internal_error;
+    const int64_t groups = (nrhs + NRC - 1) / NRC;
+    k<<<(unsigned)(bc * groups), 256, smem, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip);
+    return launch_status();
+}
+
+template <typename T>
+rocblas_status launch_getrs(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A, int lda,
+                            const int* ipiv, int64_t sP, Batch<T> B, int ldb, const int* skip,
+                            int bc)
+{
+    if(n <= 8)
+        getrs_warp_nrc<T, 8>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+    else if(n <= 16)
+        getrs_warp_nrc<T, 16>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+    else if(n <= 32)
+        getrs_warp_nrc<T, 32>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+    else if(n <= 4096)
+        return nrhs == 1
+                   ? run_getrs_cta<T, 1>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc)
+                   : run_getrs_cta<T, 4>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+    else
+        return rocblas_status_not_implemented;
+    return launch_status();
+}
+
+// ------------------------------------------------------------------------------ gesv
+template <typename T, int NMAX>
+static void run_gesv_warp(cudaStream_t s, int n, int nrhs, Batch<T> A, int lda, int* ipiv,
+                          int64_t sP, Batch<T> B, int ldb, int* info, int bc)
+{
+    dim3 grid((bc + SMALL_WPB - 1) / SMALL_WPB);
+    if(nrhs == 1)
+        gesv_warp_kernel<T, NMAX, 1><<<grid, 32 * SMALL_WPB, 0, s>>>(n, nrhs, A, lda, ipiv, sP,
+                                                                      B, ldb, info, bc);
+    else
+        gesv_warp_kernel<T, NMAX, 4><<<grid, 32 * SMALL_WPB, 0, s>>>(n, nrhs, A, lda, ipiv, sP,
+                                                                      B, ldb, info, bc);
+}
+
+template <typename T>
+rocblas_status launch_gesv(cudaStream_t s, int n, int nrhs, Batch<T> A, int lda, int* ipiv,
+                           int64_t sP, Batch<T> B, int ldb, int* info, int bc)
+{
+    if(n <= 32)
+    {
+        if(n <= 8)
+            run_gesv_warp<T, 8>(s, n, nrhs, A, lda, ipiv, sP, B, ldb, info, bc);
+        else if(n <= 16)
+            run_gesv_warp<T, 16>(s, n, nrhs, A, lda, ipiv, sP, B, ldb, info, bc);
+        else
+            run_gesv_warp<T, 32>(s, n, nrhs, A, lda, ipiv, sP, B, ldb, info, bc);
+        return launch_status();
+    }
+    rocblas_status st = launch_getrf<T>(s, n, n, A, lda, ipiv, sP, info, bc, true);
+    if(st != rocblas_status_success)
+        return st;
+    return launch_getrs<T>(s, 0, n, nrhs, A, lda, ipiv, sP, B, ldb, info, bc);
+}
+
+// ------------------------------------------------------------------------------ potrf
+template <typename T, int NT, int R, int JB, int TN>
+static rocblas_status run_potrf(cudaStream_t s, int upper, int n, Batch<T> A, int lda,
+                                int* info, int bc)
+{
+    size_t smem = sizeof(T) * 2 * JB;
+    if(n > JB)
+        smem += sizeof(T) * (size_t)R * NT * (JB + 1);
+    auto k = potrf_cta_kernel<T, NT, R, JB, TN>;
+    if(!set_smem(k, smem))
+        return rocblas_status_internal_error;
+    k<<<bc, NT, smem, s>>>(upper, n, A, lda, info);
+    return launch_status();
+}
+
+template <typename T>
+rocblas_status launch_potrf(cudaStream_t s, int upper, int n, Batch<T> A, int lda, int* info,
+                            int bc)
+{
+    if(n <= 32)
+        return run_potrf<T, 32, 1, 32, 8>(s, upper, n, A, lda, info, bc);
+    if(n <= 64)
+        return run_potrf<T, 64, 1, 64, 8>(s, upper, n, A, lda, info, bc);
+    if(n <= 256)
+        return run_potrf<T, 256, 1, 32, 8>(s, upper, n, A, lda, info, bc);
+    if(n <= 512)
+        return run_potrf<T, 256, 2, 16, 8>(s, upper, n, A, lda, info, bc);
+    if(n <= 1024)
+        return run_potrf<T, 256, 4, 8, 4>(s, upper, n, A, lda, info, bc);
+    if(n <= MAX_CTA_ROWS)
+        return run_potrf<T, 256, 8, 4, 4>(s, upper, n, A, lda, info, bc);
+    return rocblas_status_not_implemented;
+}
+
+template <typename T, int NRC>
+static rocblas_status run_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A,
+                                int lda, Batch<T> B, int ldb, const int* skip, int bc)
+{
+    const size_t smem = sizeof(T) * (size_t)n * NRC;
+    auto k = potrs_cta_kernel<T, 256, NRC>;
+    if(!set_smem(k, smem))
+        return rocblas_status_internal_error;
+    const int64_t groups = (nrhs + NRC - 1) / NRC;
+    k<<<(unsigned)(bc * groups), 256, smem, s>>>(upper, n, nrhs, A, lda, B, ldb, skip);
+    return launch_status();
+}
+
+template <typename T>
+rocblas_status launch_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A, int lda,
+                            Batch<T> B, int ldb, const int* skip, int bc)
+{
+    if(n > 4096)
+        return rocblas_status_not_implemented;
+    return nrhs == 1 ? run_potrs<T, 1>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc)
+                     : run_potrs<T, 4>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
+}
+
+// ------------------------------------------------------------------------------ instances
+#define RSB_INST(T)                                                                          \
+    template rocblas_status launch_getrf<T>(cudaStream_t, int, int, Batch<T>, int, int*,   \
+                                            int64_t, int*, int, bool);                     \
+    template rocblas_status launch_getrs<T>(cudaStream_t, int, int, int, Batch<T>, int,    \
+                                            const int*, int64_t, Batch<T>, int, const int*, \
+                                            int);                                          \
+    template rocblas_status launch_gesv<T>(cudaStream_t, int, int, Batch<T>, int, int*,    \
+                                           int64_t, Batch<T>, int, int*, int);             \
+    template rocblas_status launch_potrf<T>(cudaStream_t, int, int, Batch<T>, int, int*,   \
+                                            int);                                          \
+    template rocblas_status launch_potrs<T>(cudaStream_t, int, int, int, Batch<T>, int,    \
+                                            Batch<T>, int, const int*, int);
+RSB_INST(float)
+RSB_INST(double)
+
+} // namespace rsb

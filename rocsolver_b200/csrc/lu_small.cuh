@@ -1,0 +1,356 @@
+// lu_small.cuh -- warp-per-matrix LU, triangular solve and fused gesv for m, n <= 32.
+//
+// Replaces the reference's getf2_small_kernel (specialized/roclapack_getf2_specialized_kernels.hpp:22-136,
+// one thread per row with the pivot scanned serially by every thread through LDS and
+// 3 barriers per column) and its substitution kernels for the small-n path
+// (specialized/roclapack_trsm_specialized_kernels.hpp:167-623).
+//
+// B200 design: one 32-lane warp owns one matrix, lane i holds row i in registers.  The
+// pivot search is a warp reduction with redux.sync (no shared-memory scan, no CTA
+// barrier); the row interchange is a relabelling of the lanes (no data moves); the pivot
+// row is broadcast through a double-buffered shared-memory row, ordered by __syncwarp.
+// Four independent matrices share a 128-thread CTA.
+#pragma once
+
+#include "common.cuh"
+
+namespace rsb {
+
+constexpr int SMALL_WPB = 4; // matrices (warps) per CTA
+
+// getrf for m <= 32, n <= NMAX (NMAX <= 32).  Writes LU, ipiv (1-based, PIVOT only)
+// and info.
+template <typename T, int NMAX, bool PIVOT>
+__global__ void __launch_bounds__(32 * SMALL_WPB)
+    getrf_warp_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
+                      int bc)
+{
+    __shared__ T srow[SMALL_WPB][2][NMAX];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = (int64_t)blockIdx.x * SMALL_WPB + warp;
+    if(b >= bc)
+        return;
+    T* a = A.at(b);
+    T r[NMAX];
+#pragma unroll
+    for(int j = 0; j < NMAX; ++j)
+        r[j] = (lane < m && j < n) ? a[ix(lane, j, lda)] : T(0);
+
+    int myrow = lane;
+    int mypiv = lane + 1;
+    int inf = 0;
+    const int mn = min(m, n);
+#pragma unroll
+    for(int k = 0; k < NMAX; ++k)
+    {
+        if(k < mn)
+        {
+            const int buf = k & 1;
+            int prow = k;
+            if(PIVOT)
+            {
+                typename KeyOf<T>::type kk;
+                prow = warp_argmax(pivot_key(r[k], myrow == k), myrow, lane < m && myrow >= k,
+                                   &kk);
+            }
+            if(myrow == prow)
+            {
+#pragma unroll
+                for(int j = k; j < NMAX; ++j)
+                    srow[warp][buf][j] = r[j];
+            }
+            __syncwarp();
+            const T piv = srow[warp][buf][k];
+            if(lane == k)
+                mypiv = prow + 1;
+            if(piv == T(0) && inf == 0)
+                inf = k + 1;
+            if(PIVOT)
+            {
+                if(myrow == prow)
+                    myrow = k;
+                else if(myrow == k)
+                    myrow = prow;
+            }
+            Scaler<T> s;
+            s.init(piv);
+            if(lane < m && myrow > k)
+            {
+                const T l = s.apply(r[k]);
+                r[k] = l;
+#pragma unroll
+                for(int j = k + 1; j < NMAX; ++j)
+                    r[j] = fma(-l, srow[warp][buf][j], r[j]);
+            }
+        }
+    }
+    if(lane < m)
+    {
+#pragma unroll
+        for(int j = 0; j < NMAX; ++j)
+            if(j < n)
+                a[ix(myrow, j, lda)] = r[j];
+    }
+    if(PIVOT && lane < mn)
+        ipiv[b * strideP + lane] = mypiv;
+    if(lane == 0)
+        info[b] = inf;
+}
+
+// Source-row map of the row interchanges ipiv[0..n-1]: after applying the swaps in order
+// (LAPACK dlaswp, incx = 1) position i holds original row src (returned for lane i).
+__device__ __forceinline__ int warp_perm_src(const int* piv, int n, int lane)
+{
+    const unsigned full = 0xffffffffu;
+    int pv = lane < n ? piv[lane] - 1 : lane;
+    int src = lane;
+    for(int k = 0; k < n; ++k)
+    {
+        int p = __shfl_sync(full, pv, k);
+        if(p != k)
+        {
+            int vk = __shfl_sync(full, src, k);
+            int vp = __shfl_sync(full, src, p);
+            if(lane == k)
+                src = vp;
+            else if(lane == p)
+                src = vk;
+        }
+    }
+    return src;
+}
+
+// getrs for n <= NMAX <= 32 (library/src/lapack/roclapack_getrs.hpp:117-150 order:
+// laswp, L (unit), U; or U', L' (unit), laswp backwards).  One warp per (matrix, group
+// of NRC right-hand sides).  trans == 0: lane i holds row i of LU; trans != 0: lane i
+// holds column i, so that both sweeps only need shuffles of the solved unknown.
+template <typename T, int NMAX, int NRC>
+__global__ void __launch_bounds__(32 * SMALL_WPB)
+    getrs_warp_kernel(int trans, int n, int nrhs, Batch<T> A, int lda, const int* ipiv,
+                      int64_t strideP, Batch<T> B, int ldb, const int* skip_info, int bc)
+{
+    const unsigned full = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int groups = (nrhs + NRC - 1) / NRC;
+    const int64_t task = (int64_t)blockIdx.x * SMALL_WPB + warp;
+    if(task >= (int64_t)bc * groups)
+        return;
+    const int64_t b = task / groups;
+    const int c0 = (int)(task % groups) * NRC;
+    if(skip_info && skip_info[b] != 0)
+        return;
+    const T* a = A.at(b);
+    T* x = B.at(b);
+    T r[NMAX];
+#pragma unroll
+    for(int j = 0; j < NMAX; ++j)
+        r[j] = (lane < n && j < n) ? (trans ? a[ix(j, lane, lda)] : a[ix(lane, j, lda)]) : T(0);
+    const int src = ipiv ? warp_perm_src(ipiv + b * strideP, n, lane) : lane;
+
+    T v[NRC];
+#pragma unroll
+    for(int c = 0; c < NRC; ++c)
+        v[c] = (lane < n && c0 + c < nrhs) ? x[ix(trans ? lane : src, c0 + c, ldb)] : T(0);
+
+    if(!trans)
+    {
+        // L y = P b (unit lower, column-oriented as reference dtrsm)
+#pragma unroll
+        for(int k = 0; k < NMAX; ++k)
+        {
+            if(k < n)
+            {
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                {
+                    T yk = __shfl_sync(full, v[c], k);
+                    if(lane > k)
+                        v[c] = fma(-r[k], yk, v[c]);
+                }
+            }
+        }
+        // U x = y
+#pragma unroll
+        for(int k = NMAX - 1; k >= 0; --k)
+        {
+            if(k < n)
+            {
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                {
+                    if(lane == k)
+                        v[c] = v[c] / r[k];
+                    T xk = __shfl_sync(full, v[c], k);
+                    if(lane < k)
+                        v[c] = fma(-r[k], xk, v[c]);
+                }
+            }
+        }
+    }
+    else
+    {
+        // U' y = b: lane i holds column i of U, so (U')(i,k) = U(k,i) = r[k] on lane i
+#pragma unroll
+        for(int k = 0; k < NMAX; ++k)
+        {
+            if(k < n)
+            {
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                {
+                    if(lane == k)
+                        v[c] = v[c] / r[k];
+                    T yk = __shfl_sync(full, v[c], k);
+                    if(lane > k)
+                        v[c] = fma(-r[k], yk, v[c]);
+                }
+            }
+        }
+        // L' x = y (unit)
+#pragma unroll
+        for(int k = NMAX - 1; k >= 0; --k)
+        {
+            if(k < n)
+            {
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                {
+                    T xk = __shfl_sync(full, v[c], k);
+                    if(lane < k)
+                        v[c] = fma(-r[k], xk, v[c]);
+                }
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for(int c = 0; c < NRC; ++c)
+        if(lane < n && c0 + c < nrhs)
+            x[ix(trans ? src : lane, c0 + c, ldb)] = v[c];
+}
+
+// Fused gesv for n <= NMAX <= 32: factor in registers, then solve with the factors still
+// in registers (no re-read of LU).  B is written only where info == 0, which is the
+// reference's contract (library/src/lapack/roclapack_gesv.hpp:163-176 restores B for
+// failed members).
+template <typename T, int NMAX, int NRC>
+__global__ void __launch_bounds__(32 * SMALL_WPB)
+    gesv_warp_kernel(int n, int nrhs, Batch<T> A, int lda, int* ipiv, int64_t strideP,
+                     Batch<T> B, int ldb, int* info, int bc)
+{
+    const unsigned full = 0xffffffffu;
+    __shared__ T srow[SMALL_WPB][2][NMAX];
+    __shared__ int sown[SMALL_WPB][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = (int64_t)blockIdx.x * SMALL_WPB + warp;
+    if(b >= bc)
+        return;
+    T* a = A.at(b);
+    T r[NMAX];
+#pragma unroll
+    for(int j = 0; j < NMAX; ++j)
+        r[j] = (lane < n && j < n) ? a[ix(lane, j, lda)] : T(0);
+    int myrow = lane;
+    int mypiv = lane + 1;
+    int inf = 0;
+#pragma unroll
+    for(int k = 0; k < NMAX; ++k)
+    {
+        if(k < n)
+        {
+            const int buf = k & 1;
+            typename KeyOf<T>::type kk;
+            const int prow = warp_argmax(pivot_key(r[k], myrow == k), myrow,
+                                         lane < n && myrow >= k, &kk);
+            if(myrow == prow)
+            {
+#pragma unroll
+                for(int j = k; j < NMAX; ++j)
+                    srow[warp][buf][j] = r[j];
+            }
+            __syncwarp();
+            const T piv = srow[warp][buf][k];
+            if(lane == k)
+                mypiv = prow + 1;
+            if(piv == T(0) && inf == 0)
+                inf = k + 1;
+            if(myrow == prow)
+                myrow = k;
+            else if(myrow == k)
+                myrow = prow;
+            Scaler<T> s;
+            s.init(piv);
+            if(lane < n && myrow > k)
+            {
+                const T l = s.apply(r[k]);
+                r[k] = l;
+#pragma unroll
+                for(int j = k + 1; j < NMAX; ++j)
+                    r[j] = fma(-l, srow[warp][buf][j], r[j]);
+            }
+        }
+    }
+    if(lane < n)
+    {
+#pragma unroll
+        for(int j = 0; j < NMAX; ++j)
+            if(j < n)
+                a[ix(myrow, j, lda)] = r[j];
+        ipiv[b * strideP + lane] = mypiv;
+        sown[warp][myrow] = lane;
+    }
+    if(lane == 0)
+        info[b] = inf;
+    if(inf != 0)
+        return; // uniform: B stays untouched
+    __syncwarp();
+    T* x = B.at(b);
+    for(int c0 = 0; c0 < nrhs; c0 += NRC)
+    {
+        // lane holds original row `lane` of B, which is position myrow of P*B
+        T v[NRC];
+#pragma unroll
+        for(int c = 0; c < NRC; ++c)
+            v[c] = (lane < n && c0 + c < nrhs) ? x[ix(lane, c0 + c, ldb)] : T(0);
+#pragma unroll
+        for(int k = 0; k < NMAX; ++k)
+        {
+            if(k < n)
+            {
+                const int o = sown[warp][k];
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                {
+                    T yk = __shfl_sync(full, v[c], o);
+                    if(lane < n && myrow > k)
+                        v[c] = fma(-r[k], yk, v[c]);
+                }
+            }
+        }
+#pragma unroll
+        for(int k = NMAX - 1; k >= 0; --k)
+        {
+            if(k < n)
+            {
+                const int o = sown[warp][k];
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                {
+                    if(lane == o)
+                        v[c] = v[c] / r[k];
+                    T xk = __shfl_sync(full, v[c], o);
+                    if(lane < n && myrow < k)
+                        v[c] = fma(-r[k], xk, v[c]);
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for(int c = 0; c < NRC; ++c)
+            if(lane < n && c0 + c < nrhs)
+                x[ix(myrow, c0 + c, ldb)] = v[c];
+        __syncwarp();
+    }
+}
+
+} // namespace rsb

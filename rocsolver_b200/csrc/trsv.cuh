@@ -1,0 +1,226 @@
+// trsv.cuh -- CTA-per-matrix blocked triangular solves with several right-hand sides,
+// used by getrs (n > 32), potrs and the solve adjoint.
+//
+// Replaces the reference's rocsolver_trsm_lower/upper drivers
+// (specialized/roclapack_trsm_specialized_kernels.hpp:755-997, 1007-1249: a substitution
+// kernel per diagonal block plus a rocBLAS GEMM per off-diagonal block, several launches
+// per sweep) and laswp (auxiliary/rocauxiliary_laswp.hpp:18-64).
+//
+// One CTA per (matrix, group of NRC right-hand sides); the right-hand sides live in
+// shared memory for the whole solve.  A sweep walks 32-wide diagonal blocks: warp 0
+// solves the block with shuffles (no barrier), then all threads apply the block to the
+// remaining rows (a GEMV reading the factor once, coalesced along its columns).
+// A triangular operand is addressed as M(r, c) = base[r*rs + c*cs], so transposes are
+// a swap of (rs, cs).
+#pragma once
+
+#include "common.cuh"
+
+namespace rsb {
+
+template <typename T>
+struct TriView
+{
+    const T* p;
+    int64_t rs, cs;
+    __device__ __forceinline__ T operator()(int r, int c) const
+    {
+        return p[(int64_t)r * rs + (int64_t)c * cs];
+    }
+};
+
+// Solve M x = b in place for the nc columns of sb (ld = n).  forward: M lower
+// (substitution top-down), else M upper (bottom-up).  unit: unit diagonal.
+// Must be called by all NT threads of the CTA.
+template <typename T, int NT, int NRC>
+__device__ void block_sweep(bool forward, bool unit, TriView<T> M, int n, T* sb, int nc)
+{
+    const unsigned full = 0xffffffffu;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nblk = (n + 31) / 32;
+    for(int bi = 0; bi < nblk; ++bi)
+    {
+        const int kb = forward ? bi * 32 : (nblk - 1 - bi) * 32;
+        const int nb = min(32, n - kb);
+        if(warp == 0)
+        {
+            T x[NRC];
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                x[c] = (lane < nb && c < nc) ? sb[kb + lane + c * n] : T(0);
+            if(forward)
+            {
+                for(int k = 0; k < nb; ++k)
+                {
+                    const T mlk = lane > k && lane < nb ? M(kb + lane, kb + k) : T(0);
+                    const T dkk = unit ? T(1) : M(kb + k, kb + k);
+#pragma unroll
+                    for(int c = 0; c < NRC; ++c)
+                    {
+                        if(!unit && lane == k)
+                            x[c] = x[c] / dkk;
+                        const T xk = __shfl_sync(full, x[c], k);
+                        if(lane > k && lane < nb)
+                            x[c] = fma(-mlk, xk, x[c]);
+                    }
+                }
+            }
+            else
+            {
+                for(int k = nb - 1; k >= 0; --k)
+                {
+                    const T mlk = lane < k ? M(kb + lane, kb + k) : T(0);
+                    const T dkk = unit ? T(1) : M(kb + k, kb + k);
+#pragma unroll
+                    for(int c = 0; c < NRC; ++c)
+                    {
+                        if(!unit && lane == k)
+                            x[c] = x[c] / dkk;
+                        const T xk = __shfl_sync(full, x[c], k);
+                        if(lane < k)
+                            x[c] = fma(-mlk, xk, x[c]);
+                    }
+                }
+            }
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                if(lane < nb && c < nc)
+                    sb[kb + lane + c * n] = x[c];
+        }
+        __syncthreads();
+        // rows outside the block: forward -> below it, backward -> above it
+        const int r0 = forward ? kb + nb : 0;
+        const int r1 = forward ? n : kb;
+        for(int i = r0 + tid; i < r1; i += NT)
+        {
+            T acc[NRC];
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                acc[c] = c < nc ? sb[i + c * n] : T(0);
+            for(int k = 0; k < nb; ++k)
+            {
+                const T mik = M(i, kb + k);
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                    acc[c] = fma(-mik, sb[kb + k + c * n], acc[c]);
+            }
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                if(c < nc)
+                    sb[i + c * n] = acc[c];
+        }
+        __syncthreads();
+    }
+}
+
+// Source map of LAPACK dlaswp(k1=1, k2=n, incx=1): position i receives original row
+// perm[i].  Serial in the swap order (each interchange depends on the previous ones).
+__device__ __forceinline__ void build_perm(const int* piv, int n, int* perm)
+{
+    for(int i = threadIdx.x; i < n; i += blockDim.x)
+        perm[i] = i;
+    __syncthreads();
+    if(threadIdx.x == 0)
+    {
+        for(int k = 0; k < n; ++k)
+        {
+            const int p = piv[k] - 1;
+            if(p != k)
+            {
+                const int t = perm[k];
+                perm[k] = perm[p];
+                perm[p] = t;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// getrs for any n: trans == 0: P b, L (unit) forward, U backward;
+// trans != 0: U' forward, L' (unit) backward, P' x.
+// (library/src/lapack/roclapack_getrs.hpp:117-150)
+template <typename T, int NT, int NRC>
+__global__ void __launch_bounds__(NT)
+    getrs_cta_kernel(int trans, int n, int nrhs, Batch<T> A, int lda, const int* ipiv,
+                     int64_t strideP, Batch<T> B, int ldb, const int* skip_info)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sb = reinterpret_cast<T*>(smem_raw);
+    int* perm = reinterpret_cast<int*>(sb + (size_t)n * NRC);
+    const int groups = (nrhs + NRC - 1) / NRC;
+    const int64_t b = blockIdx.x / groups;
+    const int c0 = (blockIdx.x % groups) * NRC;
+    const int nc = min(NRC, nrhs - c0);
+    if(skip_info && skip_info[b] != 0)
+        return;
+    const T* a = A.at(b);
+    T* x = B.at(b);
+    const bool pv = ipiv != nullptr;
+    if(pv)
+        build_perm(ipiv + b * strideP, n, perm);
+    for(int e = threadIdx.x; e < n * nc; e += NT)
+    {
+        const int i = e % n, c = e / n;
+        const int src = (!trans && pv) ? perm[i] : i;
+        sb[i + c * n] = x[ix(src, c0 + c, ldb)];
+    }
+    __syncthreads();
+    if(!trans)
+    {
+        block_sweep<T, NT, NRC>(true, true, TriView<T>{a, 1, lda}, n, sb, nc);
+        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc);
+    }
+    else
+    {
+        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc);
+        block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sb, nc);
+    }
+    for(int e = threadIdx.x; e < n * nc; e += NT)
+    {
+        const int i = e % n, c = e / n;
+        const int dst = (trans && pv) ? perm[i] : i;
+        x[ix(dst, c0 + c, ldb)] = sb[i + c * n];
+    }
+}
+
+// potrs for any n: A = L L' (lower) or U' U (upper)
+// (library/src/lapack/roclapack_potrs.hpp:87-152).
+template <typename T, int NT, int NRC>
+__global__ void __launch_bounds__(NT)
+    potrs_cta_kernel(int upper, int n, int nrhs, Batch<T> A, int lda, Batch<T> B, int ldb,
+                     const int* skip_info)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sb = reinterpret_cast<T*>(smem_raw);
+    const int groups = (nrhs + NRC - 1) / NRC;
+    const int64_t b = blockIdx.x / groups;
+    const int c0 = (blockIdx.x % groups) * NRC;
+    const int nc = min(NRC, nrhs - c0);
+    if(skip_info && skip_info[b] != 0)
+        return;
+    const T* a = A.at(b);
+    T* x = B.at(b);
+    for(int e = threadIdx.x; e < n * nc; e += NT)
+    {
+        const int i = e % n, c = e / n;
+        sb[i + c * n] = x[ix(i, c0 + c, ldb)];
+    }
+    __syncthreads();
+    if(!upper)
+    {
+        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, 1, lda}, n, sb, nc);
+        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, lda, 1}, n, sb, nc);
+    }
+    else
+    {
+        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc);
+        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc);
+    }
+    for(int e = threadIdx.x; e < n * nc; e += NT)
+    {
+        const int i = e % n, c = e / n;
+        x[ix(i, c0 + c, ldb)] = sb[i + c * n];
+    }
+}
+
+} // namespace rsb

@@ -1,0 +1,152 @@
+"""Generate the golden LAPACK fixtures that pin the oracle.
+
+The reference keeps no golden vectors: its tests run host LAPACK at test time
+(clients/common/lapack_host_reference.cpp:5052-5392).  Reference-LAPACK 3.9.1
+(install.sh:182) is not installed here; the LAPACK that is, is OpenBLAS as
+bundled with scipy (scipy.linalg.lapack).  This script runs it on
+
+  * the reference's own test inputs (mt19937(69069) integers 1..10, +400 on the
+    diagonal and -4 off it, rows reversed, zeroed columns in the "singular"
+    members; clients/include/testing_getf2_getrf.hpp:128-180,
+    testing_getrs.hpp:125-160, testing_potf2_potrf.hpp:103-140,
+    testing_gesv.hpp:138-180) over the sizes of the reference's check-in
+    suites (clients/gtest/getf2_getrf_gtest.cpp:24-56, getrs_gtest.cpp,
+    potf2_potrf_gtest.cpp, potrs_gtest.cpp, gesv_gtest.cpp, posv_gtest.cpp);
+  * uniform[-1,1] matrices at the sizes of the benchmarked configurations
+    (scaled down in batch), and edge sizes n = 1, 2, 31, 33, 63, 65;
+
+and stores the LAPACK outputs in lapack_golden.npz (the inputs are regenerated
+from the same seeded generators in tests/refcases.py).  Run it with
+``python tests/golden/make_golden.py`` from the repository root.
+"""
+import os
+import sys
+
+import numpy as np
+import scipy.linalg.lapack as la
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from tests.refcases import (ref_getrf_input, ref_getrs_input, ref_potrf_input,  # noqa: E402
+                            ref_gesv_input, uniform_general, spd_gram)
+
+BC = 3  # batched variants of the reference suites use batch_count = 3
+
+
+def lapack_getrf(A):
+    lu, piv, info = la.dgetrf(A, overwrite_a=0)
+    return lu, (piv + 1).astype(np.int32), int(info)
+
+
+def lapack_potrf(A, lower):
+    c, info = la.dpotrf(A, lower=int(lower), clean=0, overwrite_a=0)
+    return c, int(info)
+
+
+def main():
+    out = {}
+    cases = []
+
+    # ---- getrf: reference suite sizes (m x n), lda = m, regular + singular
+    for m in (32, 50, 70):
+        for n in (16, 20, 40, 100):
+            for singular in (False, True):
+                A = ref_getrf_input(m, n, m, BC, singular)
+                key = f"getrf_ref_m{m}_n{n}_s{int(singular)}"
+                lus, pivs, infos = [], [], []
+                for b in range(BC):
+                    lu, piv, info = lapack_getrf(A[b])
+                    lus.append(lu); pivs.append(piv); infos.append(info)
+                out[key + "_LU"] = np.stack(lus)
+                out[key + "_ipiv"] = np.stack(pivs)
+                out[key + "_info"] = np.array(infos, np.int32)
+                cases.append(key)
+
+    # ---- getrf: uniform[-1,1], square and edge sizes
+    for n in (1, 2, 5, 31, 32, 33, 63, 64, 65, 100, 128):
+        A = uniform_general(n, n, 4, seed=100 + n)
+        key = f"getrf_uni_n{n}"
+        lus, pivs, infos = [], [], []
+        for b in range(A.shape[0]):
+            lu, piv, info = lapack_getrf(A[b])
+            lus.append(lu); pivs.append(piv); infos.append(info)
+        out[key + "_LU"] = np.stack(lus)
+        out[key + "_ipiv"] = np.stack(pivs)
+        out[key + "_info"] = np.array(infos, np.int32)
+        cases.append(key)
+
+    # ---- getrs: reference suite (n x nrhs, trans N/T)
+    for n in (20, 30, 50):
+        for nrhs in (10, 20, 30):
+            A, B = ref_getrs_input(n, nrhs, BC)
+            for trans in (0, 1):
+                key = f"getrs_ref_n{n}_r{nrhs}_t{trans}"
+                lus, pivs, xs = [], [], []
+                for b in range(BC):
+                    lu, piv, info = lapack_getrf(A[b])
+                    x, info2 = la.dgetrs(lu, piv - 1, B[b], trans=trans)
+                    assert info2 == 0
+                    lus.append(lu); pivs.append(piv); xs.append(x)
+                out[key + "_LU"] = np.stack(lus)
+                out[key + "_ipiv"] = np.stack(pivs)
+                out[key + "_X"] = np.stack(xs)
+                cases.append(key)
+
+    # ---- potrf: reference suite (n in 10,20,50,70), uplo L/U, regular + singular
+    for n in (10, 20, 50, 70):
+        for lower in (True, False):
+            for singular in (False, True):
+                A = ref_potrf_input(n, BC, singular)
+                key = f"potrf_ref_n{n}_L{int(lower)}_s{int(singular)}"
+                cs, infos = [], []
+                for b in range(BC):
+                    c, info = lapack_potrf(A[b], lower)
+                    cs.append(c); infos.append(info)
+                out[key + "_C"] = np.stack(cs)
+                out[key + "_info"] = np.array(infos, np.int32)
+                cases.append(key)
+
+    # ---- potrf / potrs on SPD Gram matrices (configuration shape n=64, nrhs=4)
+    for n in (1, 2, 31, 33, 64, 65):
+        A = spd_gram(n, 4, seed=200 + n)
+        rng = np.random.default_rng(300 + n)
+        B = rng.standard_normal((4, n, 4))
+        for lower in (True, False):
+            key = f"potrs_spd_n{n}_L{int(lower)}"
+            cs, xs, infos = [], [], []
+            for b in range(4):
+                c, info = lapack_potrf(A[b], lower)
+                x, info2 = la.dpotrs(c, B[b], lower=int(lower))
+                cs.append(c); xs.append(x); infos.append(info)
+            out[key + "_C"] = np.stack(cs)
+            out[key + "_info"] = np.array(infos, np.int32)
+            out[key + "_X"] = np.stack(xs)
+            cases.append(key)
+
+    # ---- gesv: reference suite (n, nrhs), regular + singular
+    for n in (20, 35, 50):
+        for nrhs in (1, 10):
+            for singular in (False, True):
+                A, B = ref_gesv_input(n, nrhs, BC, singular)
+                key = f"gesv_ref_n{n}_r{nrhs}_s{int(singular)}"
+                lus, pivs, xs, infos = [], [], [], []
+                for b in range(BC):
+                    lu, piv, x, info = la.dgesv(A[b], B[b])
+                    if info != 0:  # LAPACK leaves B untouched on failure
+                        x = B[b].copy()
+                    lus.append(lu); pivs.append((piv + 1).astype(np.int32)); xs.append(x)
+                    infos.append(int(info))
+                out[key + "_ipiv"] = np.stack(pivs)
+                out[key + "_X"] = np.stack(xs)
+                out[key + "_info"] = np.array(infos, np.int32)
+                cases.append(key)
+
+    out["cases"] = np.array(cases)
+    path = os.path.join(HERE, "lapack_golden.npz")
+    np.savez_compressed(path, **out)
+    print(path, len(cases), "cases", os.path.getsize(path) // 1024, "KiB")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,103 @@
+"""Input generators shared by the tests and the golden-fixture script.
+
+Matrices are returned as numpy arrays of shape (batch, rows, cols), element
+(i, j) of member b at [b, i, j].  ``to_colmajor`` packs them into the flat
+column-major (lda, stride) layout of the reference API.
+
+Reference-style generators reproduce rocSOLVER's own test inputs exactly
+(clients/include/testing_*.hpp initData functions); see oracle/refgen.cpp for
+the integer stream.
+"""
+import numpy as np
+
+
+def _refstream(count):
+    import oracle
+    return oracle.refgen(count)
+
+
+def _member_view(flat, bc, ld, ncols):
+    # flat buffer filled in memory order -> (bc, ld, ncols) with column-major members
+    return flat.reshape(bc, ncols, ld).transpose(0, 2, 1).copy()
+
+
+def ref_getrf_input(m, n, lda, bc, singular):
+    """clients/include/testing_getf2_getrf.hpp:128-180."""
+    A = _member_view(_refstream(bc * lda * n), bc, lda, n)
+    for b in range(bc):
+        for i in range(m):
+            for j in range(n):
+                A[b, i, j] += 400.0 if i == j else -4.0
+        A[b, :m, :] = A[b, :m, :][::-1, :].copy()
+        if singular and (b == bc // 4 or b == bc // 2 or b == bc - 1):
+            for j0 in (n // 4 + b, n // 2 + b, n - 1 + b):
+                A[b, :m, j0 % n] = 0.0
+    return A[:, :m, :].copy()
+
+
+def ref_getrs_input(n, nrhs, bc):
+    """clients/include/testing_getrs.hpp:125-160 (A before its host getrf, and B)."""
+    A = _member_view(_refstream(bc * n * n), bc, n, n)
+    B = _member_view(_refstream(bc * n * nrhs), bc, n, nrhs)
+    idx = np.arange(n)
+    for b in range(bc):
+        A[b] -= 4.0
+        A[b, idx, idx] += 404.0
+    return A, B
+
+
+def ref_gesv_input(n, nrhs, bc, singular):
+    """clients/include/testing_gesv.hpp:138-180."""
+    A, B = ref_getrs_input(n, nrhs, bc)
+    if singular:
+        for b in range(bc):
+            if b == bc // 4 or b == bc // 2 or b == bc - 1:
+                for j0 in (n // 4 + b, n // 2 + b, n - 1 + b):
+                    A[b, :, j0 % n] = 0.0
+    return A, B
+
+
+def ref_potrf_input(n, bc, singular):
+    """clients/include/testing_potf2_potrf.hpp:103-140 (non-symmetric; only the
+    referenced triangle matters)."""
+    A = _member_view(_refstream(bc * n * n), bc, n, n)
+    idx = np.arange(n)
+    for b in range(bc):
+        A[b, idx, idx] = A[b, idx, idx] * A[b, idx, idx] * 400.0
+        if singular and (b == bc // 4 or b == bc // 2 or b == bc - 1):
+            for i0 in (n // 4 + b, n // 2 + b, n - 1 + b):
+                A[b, i0 % n, i0 % n] = 0.0
+    return A
+
+
+def uniform_general(m, n, bc, seed, lo=-1.0, hi=1.0):
+    return np.random.default_rng(seed).uniform(lo, hi, size=(bc, m, n))
+
+
+def spd_gram(n, bc, seed):
+    """A = G G^T + n I with G ~ N(0,1) (the Cholesky configuration's inputs)."""
+    G = np.random.default_rng(seed).standard_normal((bc, n, n))
+    return G @ G.transpose(0, 2, 1) + n * np.eye(n)[None]
+
+
+def to_colmajor(A, ld=None, stride=None, dtype=None):
+    """(bc, m, n) -> flat column-major buffer with leading dimension ld and
+    member stride (elements); padding is filled with NaN so stray reads and
+    writes show up."""
+    bc, m, n = A.shape
+    ld = m if ld is None else ld
+    stride = ld * n if stride is None else stride
+    dtype = A.dtype if dtype is None else dtype
+    flat = np.full(max(stride * bc, 1), np.nan, dtype=dtype)
+    for b in range(bc):
+        blk = np.full((n, ld), np.nan, dtype=dtype)
+        blk[:, :m] = A[b].T
+        flat[b * stride: b * stride + ld * n] = blk.reshape(-1)
+    return flat
+
+
+def from_colmajor(flat, bc, m, n, ld, stride):
+    out = np.empty((bc, m, n), dtype=flat.dtype)
+    for b in range(bc):
+        out[b] = flat[b * stride: b * stride + ld * n].reshape(n, ld).T[:m, :]
+    return out
