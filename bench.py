@@ -9,6 +9,10 @@ with the inputs copied from pinned host memory and the solutions read back every
 
 Workloads (synthetic inputs with the shapes and value distributions of the reference
 configurations; no dataset is involved):
+  dsgesv_n256 (default) the mixed-precision solver rocsolver_dsgesv_strided_batched (FP32 LU +
+              FP64 iterative refinement, FP64 fallback) on the inputs of gesv_n256; value =
+              its solves/s, with the plain FP64 getrf+getrs timed on the same inputs in the
+              same run ("plain_fp64") and the backward error of every member checked.
   gesv_n256   n=256, batch 2048, nrhs 1, A = U diag(s) V' with cond log-uniform in
               [1e1, 1e6], b ~ U[-1,1]; dgetrf_strided_batched + dgetrs_strided_batched
               (plain FP64).  Metric: solves/s.
@@ -41,8 +45,8 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="gesv_n256",
-                   choices=["gesv_n256", "getrf_n32", "potrf_n64"])
+    p.add_argument("--workload", default="dsgesv_n256",
+                   choices=["dsgesv_n256", "gesv_n256", "getrf_n32", "potrf_n64"])
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target CPU time of the bounded CPU-baseline sample")
     return p.parse_args()
@@ -147,7 +151,7 @@ class Workload:
 def build_workload(name, torch, rs, dev, handle):
     w = Workload()
     w.name = name
-    if name == "gesv_n256":
+    if name in ("gesv_n256", "dsgesv_n256"):
         n, bc, nrhs = 256, 2048, 1
         A = make_cond_matrices(torch, n, bc, seed=2, device=dev)
         g = torch.Generator(device=dev)
@@ -169,6 +173,13 @@ def build_workload(name, torch, rs, dev, handle):
         w.bytes_per_unit_getrf = 2 * n * n * 8 + 4 * n + 4
         w.dominant = "getrf_cta_kernel"
         w.launches_per_step = 2
+        if name == "dsgesv_n256":
+            w.metric = ("batched solves/s at FP64 backward err <=1e-13: mixed+IR vs plain FP64 LU")
+            w.config["workload"] = ("dsgesv_strided_batched (FP32 LU + FP64 IR, <=10 iters, FP64 "
+                                    "fallback) vs plain dgetrf+dgetrs, n=256, batch=2048, nrhs=1, "
+                                    "cond log-uniform [1e1,1e6]")
+            w.dominant = "getrf_cta_kernel<float> (FP32 LU inside dsgesv)"
+            w.launches_per_step = 6
     elif name == "getrf_n32":
         n, bc, nrhs = 32, 1000, 1
         rng = np.random.default_rng(0)
@@ -302,6 +313,71 @@ def run_ours(w, torch, rs, dev, handle, steps, warmup):
             "info_nonzero": int((info_h != 0).sum())}
 
 
+def run_mixed(w, torch, rs, dev, handle, steps, warmup):
+    """dsgesv on the same inputs: per-step event pairs around the API call (A and B are
+    not modified by a converged solve; A is restored between steps anyway, outside the
+    events, in case a member fell back to FP64)."""
+    n, bc, nrhs = w.n, w.bc, w.nrhs
+    A = w.A0.clone()
+    B = w.B0.clone()
+    X = torch.empty_like(B)
+    ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
+    info = torch.zeros(bc, dtype=torch.int32, device=dev)
+    it = torch.zeros(bc, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    h = handle.value
+
+    def call():
+        rs.check(rs.call("rocsolver_dsgesv_strided_batched", h, n, nrhs, rs.ptr(A), n, n * n,
+                         rs.ptr(ipiv), n, rs.ptr(B), n, n * nrhs, rs.ptr(X), n, n * nrhs,
+                         rs.ptr(it), rs.ptr(info), bc), "dsgesv")
+
+    for _ in range(warmup):
+        A.copy_(w.A0)
+        call()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    time.sleep(0.3)
+    for i in range(steps):
+        A.copy_(w.A0)
+        ev[i][0].record(stream)
+        call()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    # FP32 LU kernel alone (the same kernel dsgesv launches), for the roofline
+    A32 = w.A0.float()
+    fev = []
+    for _ in range(min(steps, 10)):
+        Ac = A32.clone()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rs.check(rs.call("rocsolver_sgetrf_strided_batched", h, n, n, rs.ptr(Ac), n, n * n,
+                         rs.ptr(ipiv), n, rs.ptr(info), bc), "sgetrf")
+        b.record(stream)
+        fev.append((a, b))
+    torch.cuda.synchronize()
+    fact_ms = statistics.median([a.elapsed_time(b) for a, b in fev])
+    # accuracy of the last timed call: every member's backward error
+    A.copy_(w.A0)
+    call()
+    Xr = X.view(bc, nrhs, n).transpose(1, 2)
+    R = torch.bmm(w.Arow, Xr) - w.Brow
+    num = R.abs().sum(2).amax(1)
+    den = w.Arow.abs().sum(2).amax(1) * Xr.abs().sum(2).amax(1) + w.Brow.abs().sum(2).amax(1)
+    berr = num / den
+    its = it.cpu().numpy()
+    return {"step_ms": step_ms, "fact_ms": fact_ms, "clocks": clocks,
+            "berr_max": float(berr.max()), "berr_frac_1e13": float((berr <= 1e-13).double().mean()),
+            "info_nonzero": int((info.cpu().numpy() != 0).sum()),
+            "iter_mean": float(its[its >= 0].mean()) if (its >= 0).any() else None,
+            "iter_max": int(its.max()), "fallbacks": int((its < 0).sum())}
+
+
 def run_e2e(w, torch, rs, dev, handle, steps):
     """Same step through the public C ABI with host buffers: pinned A and B copied H2D,
     factor + solve, solutions and info copied D2H, every step."""
@@ -317,9 +393,19 @@ def run_e2e(w, torch, rs, dev, handle, steps):
     stream = torch.cuda.current_stream()
     h = handle.value
 
+    dX = torch.empty_like(w.B0)
+    it = torch.zeros(bc, dtype=torch.int32, device=dev)
+
     def step():
         dA.copy_(hA, non_blocking=True)
         dB.copy_(hB, non_blocking=True)
+        if w.name == "dsgesv_n256":
+            rs.check(rs.call("rocsolver_dsgesv_strided_batched", h, n, nrhs, rs.ptr(dA), n,
+                             n * n, rs.ptr(ipiv), n, rs.ptr(dB), n, n * nrhs, rs.ptr(dX), n,
+                             n * nrhs, rs.ptr(it), rs.ptr(info), bc), "dsgesv")
+            hX.copy_(dX, non_blocking=True)
+            hI.copy_(info, non_blocking=True)
+            return
         if w.name == "potrf_n64":
             rs.check(rs.call("rocsolver_dposv_strided_batched", h, rs.FILL_LOWER, n, nrhs,
                              rs.ptr(dA), n, n * n, rs.ptr(dB), n, n * nrhs, rs.ptr(info), bc),
@@ -405,7 +491,12 @@ def main():
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
-    res = run_ours(w, torch, rs, dev, handle, args.steps, args.warmup)
+    plain = None
+    if w.name == "dsgesv_n256":
+        plain = run_ours(w, torch, rs, dev, handle, args.steps, args.warmup)
+        res = run_mixed(w, torch, rs, dev, handle, args.steps, args.warmup)
+    else:
+        res = run_ours(w, torch, rs, dev, handle, args.steps, args.warmup)
     total_ms = sum(res["step_ms"])
     if pg:
         t = torch.tensor([total_ms], device=dev)
@@ -441,6 +532,23 @@ def main():
                      "frac_backward_err_le_1e-13": res["berr_frac_1e13"],
                      "info_nonzero": res["info_nonzero"]},
     }
+    if plain is not None:
+        plain_ms = sum(plain["step_ms"]) / args.steps
+        line["plain_fp64"] = {"value": units / (plain_ms / 1e3), "unit": w.unit,
+                              "ms_per_step": plain_ms, "getrf_ms": plain["fact_ms"],
+                              "backward_err_max": plain["berr_max"],
+                              "frac_backward_err_le_1e-13": plain["berr_frac_1e13"]}
+        line["mixed_over_plain"] = plain_ms / ms_per_step
+        line["accuracy"].update({"iter_mean": res["iter_mean"], "iter_max": res["iter_max"],
+                                 "fp64_fallbacks": res["fallbacks"]})
+        fbytes = (2 * w.n * w.n * 4 + 4 * w.n + 4) * w.bc
+        fgbs = fbytes / (res["fact_ms"] / 1e3) / 1e9
+        line["roofline"] = {"bound": "hbm", "kernel": w.dominant, "achieved": fgbs,
+                            "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                            "frac": fgbs / peaks["hbm_gbs"], "traffic": None,
+                            "peak_source": peaks["source"], "kernel_ms": res["fact_ms"],
+                            "fp32_tflops": w.flops_per_unit * w.bc / (res["fact_ms"] / 1e3)
+                            / 1e12}
     if rank == 0 and world == 1:
         line["cpu_baseline"] = cpu_sample(w, args.cpu_seconds)
     if rank == 0:

@@ -580,6 +580,225 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dposv_strided_batched(rocblas_handle h
     rocblas_int* info,
     const rocblas_int batch_count);
 
+/* ---- entry points with no counterpart in the reference ------------------ */
+
+/* Mixed-precision solver with iterative refinement for a strided batch (LAPACK dsgesv
+ * semantics per member; the reference has no mixed-precision gesv).  Each member is
+ * factored in FP32 (LU with partial pivoting of an FP32 copy of A), then refined in FP64:
+ * r = B - A X is formed from the FP64 A, the correction is solved with the FP32 factors,
+ * and the loop stops when every column satisfies ||r||_inf <= ||x||_inf ||A||_inf eps
+ * sqrt(n) (eps = 2^-53), after at most 10 corrections.
+ *   X (ldx >= n)  : solution; B is not modified.
+ *   iter[b] >= 0  : number of corrections; A unchanged; ipiv holds the FP32 pivots.
+ *   iter[b] < 0   : refinement failed or was skipped (-1 not attempted, -2 FP32 overflow,
+ *                   -3 FP32 factor singular, -11 no convergence in 10 corrections); the
+ *                   member was re-solved in FP64: A holds its LU factors, ipiv/info come
+ *                   from the FP64 factorisation.
+ *   info[b]       : 0, or k > 0 if U(k,k) of the FP64 factorisation is exactly zero (then
+ *                   X is not computed).
+ * Uses the handle's device workspace: 4*n*n*batch_count bytes plus O(batch_count). */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dsgesv_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    double* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    double* X,
+    const rocblas_int ldx,
+    const rocblas_stride strideX,
+    rocblas_int* iter,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* Adjoint of the batched solve X = A^{-1} B (no counterpart in the reference).  From the
+ * getrf factors of A (A, lda, strideA, ipiv, strideP as returned by getrf) and the upstream
+ * gradient G = dL/dX, computes gB = A^{-T} G and gA = -gB X^T without refactoring.
+ * gB may alias G.  X is the forward solution (ldx >= n). */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrs_adjoint_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    float* X,
+    const rocblas_int ldx,
+    const rocblas_stride strideX,
+    float* G,
+    const rocblas_int ldg,
+    const rocblas_stride strideG,
+    float* gA,
+    const rocblas_int ldga,
+    const rocblas_stride strideGA,
+    float* gB,
+    const rocblas_int ldgb,
+    const rocblas_stride strideGB,
+    const rocblas_int batch_count);
+
+/* Same for the SPD solve with potrf factors (uplo as given to potrf): gB = A^{-1} G,
+ * gA = -gB X^T (unsymmetrised gradient with respect to every entry of A). */
+ROCSOLVER_EXPORT rocblas_status rocsolver_spotrs_adjoint_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    float* X,
+    const rocblas_int ldx,
+    const rocblas_stride strideX,
+    float* G,
+    const rocblas_int ldg,
+    const rocblas_stride strideG,
+    float* gA,
+    const rocblas_int ldga,
+    const rocblas_stride strideGA,
+    float* gB,
+    const rocblas_int ldgb,
+    const rocblas_stride strideGB,
+    const rocblas_int batch_count);
+
+/* Variable-size batches in one persistent launch (no counterpart in the reference).
+ * n, nrhs, lda, ldb are DEVICE arrays of batch_count entries; A, B, ipiv are device
+ * arrays of device pointers; max_n / max_nrhs (host) bound every member and select the
+ * kernel configuration.  Members are ordered by size on the device (largest first) and
+ * pulled from a work queue; no host synchronisation, so a call can be captured into a
+ * CUDA graph once the handle's workspace is large enough (call once, or size-query and
+ * rocblas_set_workspace, before capturing).  A member whose sizes are out of range gets
+ * info = -1 and is not touched.  gesv/getrf: same per-member semantics as the
+ * fixed-size routines (square members). */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrf_vbatched(rocblas_handle handle,
+    const rocblas_int* n,
+    float* const A[],
+    const rocblas_int* lda,
+    rocblas_int* const ipiv[],
+    rocblas_int* info,
+    const rocblas_int max_n,
+    const rocblas_int batch_count);
+
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrs_vbatched(rocblas_handle handle,
+    const rocblas_int* n,
+    const rocblas_int* nrhs,
+    float* const A[],
+    const rocblas_int* lda,
+    rocblas_int* const ipiv[],
+    float* const B[],
+    const rocblas_int* ldb,
+    const rocblas_int max_n,
+    const rocblas_int max_nrhs,
+    const rocblas_int batch_count);
+
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgesv_vbatched(rocblas_handle handle,
+    const rocblas_int* n,
+    const rocblas_int* nrhs,
+    float* const A[],
+    const rocblas_int* lda,
+    rocblas_int* const ipiv[],
+    float* const B[],
+    const rocblas_int* ldb,
+    rocblas_int* info,
+    const rocblas_int max_n,
+    const rocblas_int max_nrhs,
+    const rocblas_int batch_count);
+
+/* Adjoint of the batched solve X = A^{-1} B (no counterpart in the reference).  From the
+ * getrf factors of A (A, lda, strideA, ipiv, strideP as returned by getrf) and the upstream
+ * gradient G = dL/dX, computes gB = A^{-T} G and gA = -gB X^T without refactoring.
+ * gB may alias G.  X is the forward solution (ldx >= n). */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrs_adjoint_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    double* X,
+    const rocblas_int ldx,
+    const rocblas_stride strideX,
+    double* G,
+    const rocblas_int ldg,
+    const rocblas_stride strideG,
+    double* gA,
+    const rocblas_int ldga,
+    const rocblas_stride strideGA,
+    double* gB,
+    const rocblas_int ldgb,
+    const rocblas_stride strideGB,
+    const rocblas_int batch_count);
+
+/* Same for the SPD solve with potrf factors (uplo as given to potrf): gB = A^{-1} G,
+ * gA = -gB X^T (unsymmetrised gradient with respect to every entry of A). */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dpotrs_adjoint_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    double* X,
+    const rocblas_int ldx,
+    const rocblas_stride strideX,
+    double* G,
+    const rocblas_int ldg,
+    const rocblas_stride strideG,
+    double* gA,
+    const rocblas_int ldga,
+    const rocblas_stride strideGA,
+    double* gB,
+    const rocblas_int ldgb,
+    const rocblas_stride strideGB,
+    const rocblas_int batch_count);
+
+/* Variable-size batches in one persistent launch (no counterpart in the reference).
+ * n, nrhs, lda, ldb are DEVICE arrays of batch_count entries; A, B, ipiv are device
+ * arrays of device pointers; max_n / max_nrhs (host) bound every member and select the
+ * kernel configuration.  Members are ordered by size on the device (largest first) and
+ * pulled from a work queue; no host synchronisation, so a call can be captured into a
+ * CUDA graph once the handle's workspace is large enough (call once, or size-query and
+ * rocblas_set_workspace, before capturing).  A member whose sizes are out of range gets
+ * info = -1 and is not touched.  gesv/getrf: same per-member semantics as the
+ * fixed-size routines (square members). */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrf_vbatched(rocblas_handle handle,
+    const rocblas_int* n,
+    double* const A[],
+    const rocblas_int* lda,
+    rocblas_int* const ipiv[],
+    rocblas_int* info,
+    const rocblas_int max_n,
+    const rocblas_int batch_count);
+
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetrs_vbatched(rocblas_handle handle,
+    const rocblas_int* n,
+    const rocblas_int* nrhs,
+    double* const A[],
+    const rocblas_int* lda,
+    rocblas_int* const ipiv[],
+    double* const B[],
+    const rocblas_int* ldb,
+    const rocblas_int max_n,
+    const rocblas_int max_nrhs,
+    const rocblas_int batch_count);
+
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_vbatched(rocblas_handle handle,
+    const rocblas_int* n,
+    const rocblas_int* nrhs,
+    double* const A[],
+    const rocblas_int* lda,
+    rocblas_int* const ipiv[],
+    double* const B[],
+    const rocblas_int* ldb,
+    rocblas_int* info,
+    const rocblas_int max_n,
+    const rocblas_int max_nrhs,
+    const rocblas_int batch_count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,7 +62,18 @@ _SIG = {
 }
 
 # entry points with no counterpart in the reference (declared in include/rocsolver.h)
-_EXTRA = {}
+_EXTRA = {
+    "rocsolver_dsgesv_strided_batched": (_c.c_int, [H, I, I, P, I, S, P, S, P, I, S, P, I, S, P,
+                                                    P, I]),
+}
+for _p in "sd":
+    _EXTRA[f"rocsolver_{_p}getrs_adjoint_strided_batched"] = (
+        _c.c_int, [H, I, I, P, I, S, P, S, P, I, S, P, I, S, P, I, S, P, I, S, I])
+    _EXTRA[f"rocsolver_{_p}potrs_adjoint_strided_batched"] = (
+        _c.c_int, [H, E, I, I, P, I, S, P, I, S, P, I, S, P, I, S, P, I, S, I])
+    _EXTRA[f"rocsolver_{_p}getrf_vbatched"] = (_c.c_int, [H, P, P, P, P, P, I, I])
+    _EXTRA[f"rocsolver_{_p}getrs_vbatched"] = (_c.c_int, [H, P, P, P, P, P, P, P, I, I, I])
+    _EXTRA[f"rocsolver_{_p}gesv_vbatched"] = (_c.c_int, [H, P, P, P, P, P, P, P, P, I, I, I])
 
 _HANDLE_FUNCS = {
     "rocblas_create_handle": (_c.c_int, [_c.POINTER(H)]),

@@ -1,0 +1,116 @@
+// adjoint.cu -- adjoint (reverse-mode derivative) of the batched solve X = A^{-1} B.
+//
+// No counterpart in the reference.  Given the factors the forward solve already produced
+// (getrf: P A = L U with ipiv; potrf: A = L L' or U' U) and the upstream gradient G = dL/dX:
+//   gB = A^{-T} G          (getrs with trans = T: U' solve, L' solve, inverse row swaps,
+//                           library/src/lapack/roclapack_getrs.hpp:134-150; for the SPD
+//                           case gB = A^{-1} G with the Cholesky factor)
+//   gA = -gB X^T           (rank-nrhs outer product)
+// One CTA per matrix: the right-hand sides live in shared memory through both triangular
+// sweeps, and gA is written straight from that shared-memory copy of gB, so the factors
+// are read once and gA once written; no refactorisation and no workspace.
+#include "launch.h"
+#include "trsv.cuh"
+
+namespace rsb {
+
+template <typename T, int NT, int NRC>
+__global__ void __launch_bounds__(NT)
+    solve_adjoint_kernel(int kind, int n, int nrhs, Batch<T> A, int lda, const int* ipiv,
+                         int64_t strideP, Batch<T> X, int ldx, Batch<T> G, int ldg, Batch<T> GA,
+                         int ldga, Batch<T> GB, int ldgb)
+{
+    // kind: 0 = LU (getrf factors), 1 = Cholesky lower, 2 = Cholesky upper
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sg = reinterpret_cast<T*>(smem_raw);   // n x NRC  (gB columns of the group)
+    T* sx = sg + (size_t)n * NRC;              // n x NRC  (X columns of the group)
+    int* perm = reinterpret_cast<int*>(sx + (size_t)n * NRC);
+    const int64_t b = blockIdx.x;
+    const T* a = A.at(b);
+    const T* x = X.at(b);
+    const T* g = G.at(b);
+    T* ga = GA.at(b);
+    T* gb = GB.at(b);
+    if(kind == 0)
+        build_perm(ipiv + b * strideP, n, perm);
+    for(int c0 = 0; c0 < nrhs; c0 += NRC)
+    {
+        const int nc = min(NRC, nrhs - c0);
+        for(int e = threadIdx.x; e < n * NRC; e += NT)
+        {
+            const int i = e % n, c = e / n;
+            sg[e] = c < nc ? g[ix(i, c0 + c, ldg)] : T(0);
+            sx[e] = c < nc ? x[ix(i, c0 + c, ldx)] : T(0);
+        }
+        __syncthreads();
+        if(kind == 0)
+        {
+            // A' y = g  with  A = P' L U  ->  U' L' (P y) = g
+            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sg, nc);
+            block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sg, nc);
+        }
+        else if(kind == 1)
+        {
+            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, 1, lda}, n, sg, nc);
+            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, lda, 1}, n, sg, nc);
+        }
+        else
+        {
+            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sg, nc);
+            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sg, nc);
+        }
+        // gB (inverse row interchanges for LU: gB[perm[i]] = y[i])
+        for(int e = threadIdx.x; e < n * nc; e += NT)
+        {
+            const int i = e % n, c = e / n;
+            const int dst = kind == 0 ? perm[i] : i;
+            gb[ix(dst, c0 + c, ldgb)] = sg[i + c * n];
+        }
+        // gA -= gB X' over this group: row i of gB is sg[perm^{-1}...]; address gB by its
+        // final row: for LU, final row perm[i] holds sg[i]
+        for(int e = threadIdx.x; e < n * n; e += NT)
+        {
+            const int i = e % n, j = e / n; // gA(r, j) with r = final row of sg[i]
+            const int r = kind == 0 ? perm[i] : i;
+            T acc = c0 == 0 ? T(0) : ga[ix(r, j, ldga)];
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                acc = fma(-sg[i + c * n], sx[j + c * n], acc);
+            ga[ix(r, j, ldga)] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+rocblas_status launch_solve_adjoint(cudaStream_t s, int kind, int n, int nrhs, Batch<T> A,
+                                    int lda, const int* ipiv, int64_t strideP, Batch<T> X,
+                                    int ldx, Batch<T> G, int ldg, Batch<T> GA, int ldga,
+                                    Batch<T> GB, int ldgb, int bc)
+{
+    constexpr int NT = 256;
+    constexpr int NRC = 8;
+    const size_t smem = sizeof(T) * 2 * (size_t)n * NRC + sizeof(int) * (size_t)n;
+    if(smem > 200 * 1024)
+        return rocblas_status_not_implemented;
+    auto k = solve_adjoint_kernel<T, NT, NRC>;
+    if(smem > 48 * 1024
+       && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+              != cudaSuccess)
+        return rocblas_status_internal_error;
+    k<<<bc, NT, smem, s>>>(kind, n, nrhs, A, lda, ipiv, strideP, X, ldx, G, ldg, GA, ldga, GB,
+                           ldgb);
+    return cudaGetLastError() == cudaSuccess ? rocblas_status_success
+                                             : rocblas_status_internal_error;
+}
+
+template rocblas_status launch_solve_adjoint<float>(cudaStream_t, int, int, int, Batch<float>,
+                                                    int, const int*, int64_t, Batch<float>, int,
+                                                    Batch<float>, int, Batch<float>, int,
+                                                    Batch<float>, int, int);
+template rocblas_status launch_solve_adjoint<double>(cudaStream_t, int, int, int, Batch<double>,
+                                                     int, const int*, int64_t, Batch<double>,
+                                                     int, Batch<double>, int, Batch<double>, int,
+                                                     Batch<double>, int, int);
+
+} // namespace rsb

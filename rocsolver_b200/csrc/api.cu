@@ -155,7 +155,153 @@ rocblas_status posv_impl(rocblas_handle h, rocblas_fill uplo, int n, int nrhs, B
     return launch_potrs<T>(h->stream, up, n, nrhs, A, lda, B, ldb, info, bc);
 }
 
+rocblas_status dsgesv_impl(rocblas_handle h, int n, int nrhs, double* A, int lda,
+                           int64_t strideA, int* ipiv, int64_t strideP, double* B, int ldb,
+                           int64_t strideB, double* X, int ldx, int64_t strideX, int* iter,
+                           int* info, int bc)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(n < 0 || nrhs < 0 || lda < n || ldb < n || ldx < n || bc < 0)
+        return rocblas_status_invalid_size;
+    const size_t ws_bytes = (n && nrhs && bc) ? dsgesv_workspace(n, nrhs, bc) : 0;
+    if(h->querying)
+        return ws_query(h, ws_bytes);
+    const int64_t nn = (int64_t)n * nrhs;
+    if((n && !A) || (n && !ipiv) || (nn && !B) || (nn && !X) || (bc && !info) || (bc && !iter))
+        return rocblas_status_invalid_pointer;
+    if(bc == 0)
+        return rocblas_status_success;
+    if(n == 0 || nrhs == 0)
+        return launch_reset_info2(h->stream, info, iter, bc);
+    void* ws = nullptr;
+    rocblas_status st = ws_get(h, ws_bytes, &ws);
+    if(st != rocblas_status_success)
+        return st;
+    return launch_dsgesv(h->stream, n, nrhs, strided<double>(A, strideA), lda, ipiv, strideP,
+                         strided<double>(B, strideB), ldb, strided<double>(X, strideX), ldx, iter,
+                         info, bc, ws);
+}
+
+template <typename T>
+rocblas_status adjoint_impl(rocblas_handle h, int kind, int n, int nrhs, T* A, int lda,
+                            int64_t sA, const int* ipiv, int64_t sP, T* X, int ldx, int64_t sX,
+                            T* G, int ldg, int64_t sG, T* gA, int ldga, int64_t sGA, T* gB,
+                            int ldgb, int64_t sGB, int bc)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(n < 0 || nrhs < 0 || lda < n || ldx < n || ldg < n || ldga < n || ldgb < n || bc < 0)
+        return rocblas_status_invalid_size;
+    if(h->querying)
+        return ws_query(h, 0);
+    const int64_t nn = (int64_t)n * nrhs;
+    if((n && !A) || (kind == 0 && n && !ipiv) || (nn && (!X || !G || !gB)) || (n && !gA))
+        return rocblas_status_invalid_pointer;
+    if(n == 0 || bc == 0)
+        return rocblas_status_success;
+    return launch_solve_adjoint<T>(h->stream, kind, n, nrhs, strided<T>(A, sA), lda, ipiv, sP,
+                                   strided<T>(X, sX), ldx, strided<T>(G, sG), ldg,
+                                   strided<T>(gA, sGA), ldga, strided<T>(gB, sGB), ldgb, bc);
+}
+
+template <typename T>
+rocblas_status vbatched_impl(rocblas_handle h, int mode, const int* n, const int* nrhs,
+                             T* const* A, const int* lda, int* const* ipiv, T* const* B,
+                             const int* ldb, int* info, int max_n, int max_nrhs, int bc)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(max_n < 0 || max_nrhs < 0 || bc < 0)
+        return rocblas_status_invalid_size;
+    const size_t ws_bytes = bc ? vbatched_workspace(bc) : 0;
+    if(h->querying)
+        return ws_query(h, ws_bytes);
+    if(bc && (!n || !A || !lda || !ipiv || (mode != 2 && !info)))
+        return rocblas_status_invalid_pointer;
+    if(bc && mode != 1 && (!nrhs || !B || !ldb))
+        return rocblas_status_invalid_pointer;
+    if(bc == 0)
+        return rocblas_status_success;
+    void* ws = nullptr;
+    rocblas_status st = ws_get(h, ws_bytes, &ws);
+    if(st != rocblas_status_success)
+        return st;
+    return launch_vbatched<T>(h->stream, mode, n, nrhs, A, lda, ipiv, B, ldb, info,
+                              max_n > 0 ? max_n : 1, max_nrhs, bc, ws);
+}
+
 } // namespace
+
+#define RSB_API_NEW(P, T)                                                                       \
+    rocblas_status rocsolver_##P##getrs_adjoint_strided_batched(                                \
+        rocblas_handle handle, const rocblas_int n, const rocblas_int nrhs, T* A,              \
+        const rocblas_int lda, const rocblas_stride strideA, const rocblas_int* ipiv,          \
+        const rocblas_stride strideP, T* X, const rocblas_int ldx, const rocblas_stride strideX,\
+        T* G, const rocblas_int ldg, const rocblas_stride strideG, T* gA,                      \
+        const rocblas_int ldga, const rocblas_stride strideGA, T* gB, const rocblas_int ldgb,  \
+        const rocblas_stride strideGB, const rocblas_int batch_count)                          \
+    {                                                                                           \
+        return adjoint_impl<T>(handle, 0, n, nrhs, A, lda, strideA, ipiv, strideP, X, ldx,      \
+                               strideX, G, ldg, strideG, gA, ldga, strideGA, gB, ldgb,          \
+                               strideGB, batch_count);                                          \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##potrs_adjoint_strided_batched(                                \
+        rocblas_handle handle, const rocblas_fill uplo, const rocblas_int n,                   \
+        const rocblas_int nrhs, T* A, const rocblas_int lda, const rocblas_stride strideA,     \
+        T* X, const rocblas_int ldx, const rocblas_stride strideX, T* G, const rocblas_int ldg, \
+        const rocblas_stride strideG, T* gA, const rocblas_int ldga,                           \
+        const rocblas_stride strideGA, T* gB, const rocblas_int ldgb,                          \
+        const rocblas_stride strideGB, const rocblas_int batch_count)                          \
+    {                                                                                           \
+        if(handle && bad_fill(uplo))                                                           \
+            return rocblas_status_invalid_value;                                                \
+        return adjoint_impl<T>(handle, uplo == rocblas_fill_upper ? 2 : 1, n, nrhs, A, lda,     \
+                               strideA, nullptr, 0, X, ldx, strideX, G, ldg, strideG, gA, ldga, \
+                               strideGA, gB, ldgb, strideGB, batch_count);                      \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrf_vbatched(                                               \
+        rocblas_handle handle, const rocblas_int* n, T* const A[], const rocblas_int* lda,     \
+        rocblas_int* const ipiv[], rocblas_int* info, const rocblas_int max_n,                 \
+        const rocblas_int batch_count)                                                         \
+    {                                                                                           \
+        return vbatched_impl<T>(handle, 1, n, nullptr, A, lda, ipiv, nullptr, nullptr, info,   \
+                                max_n, 0, batch_count);                                         \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##getrs_vbatched(                                               \
+        rocblas_handle handle, const rocblas_int* n, const rocblas_int* nrhs, T* const A[],    \
+        const rocblas_int* lda, rocblas_int* const ipiv[], T* const B[],                       \
+        const rocblas_int* ldb, const rocblas_int max_n, const rocblas_int max_nrhs,           \
+        const rocblas_int batch_count)                                                         \
+    {                                                                                           \
+        return vbatched_impl<T>(handle, 2, n, nrhs, A, lda, ipiv, B, ldb, nullptr, max_n,      \
+                                max_nrhs, batch_count);                                         \
+    }                                                                                           \
+    rocblas_status rocsolver_##P##gesv_vbatched(                                                \
+        rocblas_handle handle, const rocblas_int* n, const rocblas_int* nrhs, T* const A[],    \
+        const rocblas_int* lda, rocblas_int* const ipiv[], T* const B[],                       \
+        const rocblas_int* ldb, rocblas_int* info, const rocblas_int max_n,                    \
+        const rocblas_int max_nrhs, const rocblas_int batch_count)                             \
+    {                                                                                           \
+        return vbatched_impl<T>(handle, 0, n, nrhs, A, lda, ipiv, B, ldb, info, max_n,         \
+                                max_nrhs, batch_count);                                         \
+    }
+
+extern "C" {
+RSB_API_NEW(s, float)
+RSB_API_NEW(d, double)
+}
+
+extern "C" rocblas_status rocsolver_dsgesv_strided_batched(
+    rocblas_handle handle, const rocblas_int n, const rocblas_int nrhs, double* A,
+    const rocblas_int lda, const rocblas_stride strideA, rocblas_int* ipiv,
+    const rocblas_stride strideP, double* B, const rocblas_int ldb, const rocblas_stride strideB,
+    double* X, const rocblas_int ldx, const rocblas_stride strideX, rocblas_int* iter,
+    rocblas_int* info, const rocblas_int batch_count)
+{
+    return dsgesv_impl(handle, n, nrhs, A, lda, strideA, ipiv, strideP, B, ldb, strideB, X, ldx,
+                       strideX, iter, info, batch_count);
+}
 
 #define RSB_API_TYPE(P, T)                                                                      \
     rocblas_status rocsolver_##P##getrf(rocblas_handle handle, const rocblas_int m,             \

@@ -37,6 +37,26 @@ __host__ __device__ inline Batch<T> pointers(T* const* p)
     return Batch<T>{nullptr, p, 0};
 }
 
+// Per-member gate: with p == nullptr every member runs; otherwise member b runs only when
+// (p[b] != 0) == run_if_nonzero.  Used to restrict a launch to a subset of the batch (the
+// FP64 fallback of the mixed-precision solver) without compacting the batch on the host.
+struct Gate
+{
+    const int* p;
+    int run_if_nonzero;
+    __device__ __forceinline__ bool skip(int64_t b) const
+    {
+        if(!p)
+            return false;
+        const bool nz = p[b] != 0;
+        return run_if_nonzero ? !nz : nz;
+    }
+};
+__host__ __device__ inline Gate no_gate()
+{
+    return Gate{nullptr, 0};
+}
+
 __device__ __forceinline__ size_t ix(int i, int j, int ld)
 {
     return (size_t)i + (size_t)j * (size_t)ld;

@@ -14,11 +14,12 @@ namespace rsb {
 // or internal_error (launch failure).  None synchronises or allocates.
 template <typename T>
 rocblas_status launch_getrf(cudaStream_t s, int m, int n, Batch<T> A, int lda, int* ipiv,
-                            int64_t strideP, int* info, int bc, bool pivot);
+                            int64_t strideP, int* info, int bc, bool pivot,
+                            Gate gate = no_gate());
 template <typename T>
 rocblas_status launch_getrs(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A, int lda,
                             const int* ipiv, int64_t strideP, Batch<T> B, int ldb,
-                            const int* skip_info, int bc);
+                            const int* skip_info, int bc, Gate gate = no_gate());
 template <typename T>
 rocblas_status launch_gesv(cudaStream_t s, int n, int nrhs, Batch<T> A, int lda, int* ipiv,
                            int64_t strideP, Batch<T> B, int ldb, int* info, int bc);
@@ -29,6 +30,29 @@ template <typename T>
 rocblas_status launch_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A, int lda,
                             Batch<T> B, int ldb, const int* skip_info, int bc);
 rocblas_status launch_reset_info(cudaStream_t s, int* info, int bc);
+
+// mixed-precision solver (mixed.cu)
+size_t dsgesv_workspace(int n, int nrhs, int bc);
+rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, int lda,
+                             int* ipiv, int64_t strideP, Batch<double> B, int ldb,
+                             Batch<double> X, int ldx, int* iter, int* info, int bc, void* ws);
+// adjoint of the batched solve (adjoint.cu); kind 0 = LU, 1 = Cholesky lower, 2 = upper
+template <typename T>
+rocblas_status launch_solve_adjoint(cudaStream_t s, int kind, int n, int nrhs, Batch<T> A,
+                                    int lda, const int* ipiv, int64_t strideP, Batch<T> X,
+                                    int ldx, Batch<T> G, int ldg, Batch<T> GA, int ldga,
+                                    Batch<T> GB, int ldgb, int bc);
+
+// variable-size batches (vbatched.cu); mode 0 gesv, 1 getrf, 2 getrs
+size_t vbatched_workspace(int bc);
+template <typename T>
+rocblas_status launch_vbatched(cudaStream_t s, int mode, const int* n, const int* nrhs,
+                               T* const* A, const int* lda, int* const* ipiv, T* const* B,
+                               const int* ldb, int* info, int max_n, int max_nrhs, int bc,
+                               void* ws);
+
+// sets two int arrays to zero (quick returns)
+rocblas_status launch_reset_info2(cudaStream_t s, int* a, int* b, int bc);
 
 // largest m (rows) the CTA-resident LU / Cholesky kernels support
 constexpr int MAX_CTA_ROWS = 2048;

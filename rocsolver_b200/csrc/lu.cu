@@ -42,19 +42,37 @@ rocblas_status launch_reset_info(cudaStream_t s, int* info, int bc)
     return launch_status();
 }
 
+__global__ void reset_info2_kernel(int* a, int* b, int bc)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < bc)
+    {
+        a[i] = 0;
+        b[i] = 0;
+    }
+}
+
+rocblas_status launch_reset_info2(cudaStream_t s, int* a, int* b, int bc)
+{
+    if(bc <= 0)
+        return rocblas_status_success;
+    reset_info2_kernel<<<(bc + 255) / 256, 256, 0, s>>>(a, b, bc);
+    return launch_status();
+}
+
 // ------------------------------------------------------------------------------ getrf
 template <typename T, int NMAX, bool PIVOT>
 static void run_getrf_warp(cudaStream_t s, int m, int n, Batch<T> A, int lda, int* ipiv,
-                           int64_t sP, int* info, int bc)
+                           int64_t sP, int* info, int bc, Gate g)
 {
     dim3 grid((bc + SMALL_WPB - 1) / SMALL_WPB);
     getrf_warp_kernel<T, NMAX, PIVOT><<<grid, 32 * SMALL_WPB, 0, s>>>(m, n, A, lda, ipiv, sP,
-                                                                       info, bc);
+                                                                       info, bc, g);
 }
 
 template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
 static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, int lda,
-                                    int* ipiv, int64_t sP, int* info, int bc)
+                                    int* ipiv, int64_t sP, int* info, int bc, Gate g)
 {
     // U12 chunk width: multiple of TN, at most 64 KiB of shared memory
     int cw = (int)((64 * 1024) / (sizeof(T) * JB));
@@ -66,99 +84,100 @@ static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, in
     auto k = getrf_cta_kernel<T, NT, R, JB, TN, PIVOT>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
-    k<<<bc, NT, smem, s>>>(m, n, A, lda, ipiv, sP, info, cw);
+    k<<<bc, NT, smem, s>>>(m, n, A, lda, ipiv, sP, info, cw, g);
     return launch_status();
 }
 
 template <typename T, bool PIVOT>
 static rocblas_status getrf_dispatch(cudaStream_t s, int m, int n, Batch<T> A, int lda,
-                                     int* ipiv, int64_t sP, int* info, int bc)
+                                     int* ipiv, int64_t sP, int* info, int bc, Gate g)
 {
     if(m <= 32 && n <= 32)
     {
         if(n <= 8)
-            run_getrf_warp<T, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+            run_getrf_warp<T, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
         else if(n <= 16)
-            run_getrf_warp<T, 16, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+            run_getrf_warp<T, 16, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
         else
-            run_getrf_warp<T, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+            run_getrf_warp<T, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
         return launch_status();
     }
     if(m <= 64)
-        return run_getrf_cta<T, 64, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+        return run_getrf_cta<T, 64, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
     if(m <= 128)
-        return run_getrf_cta<T, 128, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+        return run_getrf_cta<T, 128, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
     if(m <= 256)
-        return run_getrf_cta<T, 256, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+        return run_getrf_cta<T, 256, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
     if(m <= 512)
-        return run_getrf_cta<T, 256, 2, 16, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+        return run_getrf_cta<T, 256, 2, 16, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
     if(m <= 1024)
-        return run_getrf_cta<T, 256, 4, 8, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+        return run_getrf_cta<T, 256, 4, 8, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
     if(m <= MAX_CTA_ROWS)
-        return run_getrf_cta<T, 256, 8, 4, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc);
+        return run_getrf_cta<T, 256, 8, 4, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
     return rocblas_status_not_implemented;
 }
 
 template <typename T>
 rocblas_status launch_getrf(cudaStream_t s, int m, int n, Batch<T> A, int lda, int* ipiv,
-                            int64_t sP, int* info, int bc, bool pivot)
+                            int64_t sP, int* info, int bc, bool pivot, Gate g)
 {
-    return pivot ? getrf_dispatch<T, true>(s, m, n, A, lda, ipiv, sP, info, bc)
-                 : getrf_dispatch<T, false>(s, m, n, A, lda, ipiv, sP, info, bc);
+    return pivot ? getrf_dispatch<T, true>(s, m, n, A, lda, ipiv, sP, info, bc, g)
+                 : getrf_dispatch<T, false>(s, m, n, A, lda, ipiv, sP, info, bc, g);
 }
 
 // ------------------------------------------------------------------------------ getrs
 template <typename T, int NMAX, int NRC>
 static void run_getrs_warp(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A, int lda,
                            const int* ipiv, int64_t sP, Batch<T> B, int ldb, const int* skip,
-                           int bc)
+                           int bc, Gate g)
 {
     const int64_t tasks = (int64_t)bc * ((nrhs + NRC - 1) / NRC);
     dim3 grid((unsigned)((tasks + SMALL_WPB - 1) / SMALL_WPB));
     getrs_warp_kernel<T, NMAX, NRC><<<grid, 32 * SMALL_WPB, 0, s>>>(trans, n, nrhs, A, lda, ipiv,
-                                                                     sP, B, ldb, skip, bc);
+                                                                     sP, B, ldb, skip, bc, g);
 }
 
 template <typename T, int NMAX>
 static void getrs_warp_nrc(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A, int lda,
                            const int* ipiv, int64_t sP, Batch<T> B, int ldb, const int* skip,
-                           int bc)
+                           int bc, Gate g)
 {
     if(nrhs == 1)
-        run_getrs_warp<T, NMAX, 1>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+        run_getrs_warp<T, NMAX, 1>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, g);
     else
-        run_getrs_warp<T, NMAX, 4>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+        run_getrs_warp<T, NMAX, 4>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, g);
 }
 
 template <typename T, int NRC>
 static rocblas_status run_getrs_cta(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A,
                                     int lda, const int* ipiv, int64_t sP, Batch<T> B, int ldb,
-                                    const int* skip, int bc)
+                                    const int* skip, int bc, Gate g)
 {
     const size_t smem = sizeof(T) * (size_t)n * NRC + sizeof(int) * (size_t)n;
     auto k = getrs_cta_kernel<T, 256, NRC>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
     const int64_t groups = (nrhs + NRC - 1) / NRC;
-    k<<<(unsigned)(bc * groups), 256, smem, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip);
+    k<<<(unsigned)(bc * groups), 256, smem, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip,
+                                                 g);
     return launch_status();
 }
 
 template <typename T>
 rocblas_status launch_getrs(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A, int lda,
                             const int* ipiv, int64_t sP, Batch<T> B, int ldb, const int* skip,
-                            int bc)
+                            int bc, Gate g)
 {
     if(n <= 8)
-        getrs_warp_nrc<T, 8>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+        getrs_warp_nrc<T, 8>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, g);
     else if(n <= 16)
-        getrs_warp_nrc<T, 16>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+        getrs_warp_nrc<T, 16>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, g);
     else if(n <= 32)
-        getrs_warp_nrc<T, 32>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+        getrs_warp_nrc<T, 32>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, g);
     else if(n <= 4096)
         return nrhs == 1
-                   ? run_getrs_cta<T, 1>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc)
-                   : run_getrs_cta<T, 4>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc);
+                   ? run_getrs_cta<T, 1>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, g)
+                   : run_getrs_cta<T, 4>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, g);
     else
         return rocblas_status_not_implemented;
     return launch_status();
@@ -258,10 +277,10 @@ rocblas_status launch_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T>
 // ------------------------------------------------------------------------------ instances
 #define RSB_INST(T)                                                                          \
     template rocblas_status launch_getrf<T>(cudaStream_t, int, int, Batch<T>, int, int*,   \
-                                            int64_t, int*, int, bool);                     \
+                                            int64_t, int*, int, bool, Gate);               \
     template rocblas_status launch_getrs<T>(cudaStream_t, int, int, int, Batch<T>, int,    \
                                             const int*, int64_t, Batch<T>, int, const int*, \
-                                            int);                                          \
+                                            int, Gate);                                    \
     template rocblas_status launch_gesv<T>(cudaStream_t, int, int, Batch<T>, int, int*,    \
                                            int64_t, Batch<T>, int, int*, int);             \
     template rocblas_status launch_potrf<T>(cudaStream_t, int, int, Batch<T>, int, int*,   \

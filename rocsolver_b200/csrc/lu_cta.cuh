@@ -42,14 +42,14 @@ struct CtaLuSmem
     }
 };
 
+// Factor one m x n matrix with the whole CTA.  smem_raw must hold CtaLuSmem::bytes(cw, R);
+// m <= R*NT.  Writes ipiv (1-based, PIVOT only) and *info_out.  Called by all threads.
 template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
-__global__ void __launch_bounds__(NT)
-    getrf_cta_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
-                     int cw)
+__device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* piv_out,
+                                              int* info_out, int cw, unsigned char* smem_raw)
 {
     using K = typename KeyOf<T>::type;
     constexpr int NW = NT / 32;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sL11 = reinterpret_cast<T*>(smem_raw);
     T* sU = sL11 + JB * JB;
     T* cand = sU + (size_t)JB * cw; // [2][NW][JB]
@@ -61,9 +61,6 @@ __global__ void __launch_bounds__(NT)
     int* nmoved = spiv + JB;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int64_t b = blockIdx.x;
-    T* a = A.at(b);
-    int* piv_out = PIVOT ? ipiv + b * strideP : nullptr;
     const int mn = min(m, n);
     int inf = 0;
 
@@ -340,7 +337,20 @@ __global__ void __launch_bounds__(NT)
         }
     }
     if(tid == 0)
-        info[b] = inf;
+        *info_out = inf;
+}
+
+template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
+__global__ void __launch_bounds__(NT)
+    getrf_cta_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
+                     int cw, Gate gate)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t b = blockIdx.x;
+    if(gate.skip(b))
+        return;
+    getrf_cta_dev<T, NT, R, JB, TN, PIVOT>(m, n, A.at(b), lda, PIVOT ? ipiv + b * strideP : nullptr,
+                                           info + b, cw, smem_raw);
 }
 
 } // namespace rsb

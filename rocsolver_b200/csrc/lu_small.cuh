@@ -23,12 +23,12 @@ constexpr int SMALL_WPB = 4; // matrices (warps) per CTA
 template <typename T, int NMAX, bool PIVOT>
 __global__ void __launch_bounds__(32 * SMALL_WPB)
     getrf_warp_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
-                      int bc)
+                      int bc, Gate gate)
 {
     __shared__ T srow[SMALL_WPB][2][NMAX];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = (int64_t)blockIdx.x * SMALL_WPB + warp;
-    if(b >= bc)
+    if(b >= bc || gate.skip(b))
         return;
     T* a = A.at(b);
     T r[NMAX];
@@ -127,7 +127,8 @@ __device__ __forceinline__ int warp_perm_src(const int* piv, int n, int lane)
 template <typename T, int NMAX, int NRC>
 __global__ void __launch_bounds__(32 * SMALL_WPB)
     getrs_warp_kernel(int trans, int n, int nrhs, Batch<T> A, int lda, const int* ipiv,
-                      int64_t strideP, Batch<T> B, int ldb, const int* skip_info, int bc)
+                      int64_t strideP, Batch<T> B, int ldb, const int* skip_info, int bc,
+                      Gate gate)
 {
     const unsigned full = 0xffffffffu;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
         return;
     const int64_t b = task / groups;
     const int c0 = (int)(task % groups) * NRC;
-    if(skip_info && skip_info[b] != 0)
+    if((skip_info && skip_info[b] != 0) || gate.skip(b))
         return;
     const T* a = A.at(b);
     T* x = B.at(b);
@@ -229,23 +230,17 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
             x[ix(trans ? src : lane, c0 + c, ldb)] = v[c];
 }
 
-// Fused gesv for n <= NMAX <= 32: factor in registers, then solve with the factors still
-// in registers (no re-read of LU).  B is written only where info == 0, which is the
-// reference's contract (library/src/lapack/roclapack_gesv.hpp:163-176 restores B for
-// failed members).
+// Fused gesv for n <= NMAX <= 32 on one warp: factor in registers, then solve with the
+// factors still in registers (no re-read of LU).  B is written only where info == 0,
+// which is the reference's contract (library/src/lapack/roclapack_gesv.hpp:163-176
+// restores B for failed members).  srow: [2][NMAX] and sown: [32] of this warp.
 template <typename T, int NMAX, int NRC>
-__global__ void __launch_bounds__(32 * SMALL_WPB)
-    gesv_warp_kernel(int n, int nrhs, Batch<T> A, int lda, int* ipiv, int64_t strideP,
-                     Batch<T> B, int ldb, int* info, int bc)
+__device__ __forceinline__ void gesv_warp_dev(int n, int nrhs, T* a, int lda, int* piv, T* x,
+                                              int ldb, int* info_out, T (*srow)[NMAX],
+                                              int* sown)
 {
     const unsigned full = 0xffffffffu;
-    __shared__ T srow[SMALL_WPB][2][NMAX];
-    __shared__ int sown[SMALL_WPB][32];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t b = (int64_t)blockIdx.x * SMALL_WPB + warp;
-    if(b >= bc)
-        return;
-    T* a = A.at(b);
+    const int lane = threadIdx.x & 31;
     T r[NMAX];
 #pragma unroll
     for(int j = 0; j < NMAX; ++j)
@@ -266,27 +261,27 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
             {
 #pragma unroll
                 for(int j = k; j < NMAX; ++j)
-                    srow[warp][buf][j] = r[j];
+                    srow[buf][j] = r[j];
             }
             __syncwarp();
-            const T piv = srow[warp][buf][k];
+            const T pivv = srow[buf][k];
             if(lane == k)
                 mypiv = prow + 1;
-            if(piv == T(0) && inf == 0)
+            if(pivv == T(0) && inf == 0)
                 inf = k + 1;
             if(myrow == prow)
                 myrow = k;
             else if(myrow == k)
                 myrow = prow;
             Scaler<T> s;
-            s.init(piv);
+            s.init(pivv);
             if(lane < n && myrow > k)
             {
                 const T l = s.apply(r[k]);
                 r[k] = l;
 #pragma unroll
                 for(int j = k + 1; j < NMAX; ++j)
-                    r[j] = fma(-l, srow[warp][buf][j], r[j]);
+                    r[j] = fma(-l, srow[buf][j], r[j]);
             }
         }
     }
@@ -296,15 +291,14 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
         for(int j = 0; j < NMAX; ++j)
             if(j < n)
                 a[ix(myrow, j, lda)] = r[j];
-        ipiv[b * strideP + lane] = mypiv;
-        sown[warp][myrow] = lane;
+        piv[lane] = mypiv;
+        sown[myrow] = lane;
     }
     if(lane == 0)
-        info[b] = inf;
+        *info_out = inf;
     if(inf != 0)
         return; // uniform: B stays untouched
     __syncwarp();
-    T* x = B.at(b);
     for(int c0 = 0; c0 < nrhs; c0 += NRC)
     {
         // lane holds original row `lane` of B, which is position myrow of P*B
@@ -317,7 +311,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
         {
             if(k < n)
             {
-                const int o = sown[warp][k];
+                const int o = sown[k];
 #pragma unroll
                 for(int c = 0; c < NRC; ++c)
                 {
@@ -332,7 +326,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
         {
             if(k < n)
             {
-                const int o = sown[warp][k];
+                const int o = sown[k];
 #pragma unroll
                 for(int c = 0; c < NRC; ++c)
                 {
@@ -351,6 +345,21 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
                 x[ix(myrow, c0 + c, ldb)] = v[c];
         __syncwarp();
     }
+}
+
+template <typename T, int NMAX, int NRC>
+__global__ void __launch_bounds__(32 * SMALL_WPB)
+    gesv_warp_kernel(int n, int nrhs, Batch<T> A, int lda, int* ipiv, int64_t strideP,
+                     Batch<T> B, int ldb, int* info, int bc)
+{
+    __shared__ T srow[SMALL_WPB][2][NMAX];
+    __shared__ int sown[SMALL_WPB][32];
+    const int warp = threadIdx.x >> 5;
+    const int64_t b = (int64_t)blockIdx.x * SMALL_WPB + warp;
+    if(b >= bc)
+        return;
+    gesv_warp_dev<T, NMAX, NRC>(n, nrhs, A.at(b), lda, ipiv + b * strideP, B.at(b), ldb, info + b,
+                                srow[warp], sown[warp]);
 }
 
 } // namespace rsb

@@ -1,0 +1,336 @@
+// mixed.cu -- mixed-precision batched solver with iterative refinement (dsgesv).
+//
+// No counterpart in the reference (rocSOLVER has no mixed-precision gesv).  Semantics are
+// LAPACK dsgesv's (the CPU analogue the reference's host oracle library provides):
+//   ITER >= 0 : refinement converged after ITER corrections, A unchanged, X solution;
+//   ITER = -2 : A, B or a residual overflows in FP32;  ITER = -3 : the FP32 LU is singular;
+//   ITER = -(ITERMAX+1): no convergence within ITERMAX corrections;
+//   ITER = -1 : refinement not attempted (shape outside the fused refinement kernel);
+//   for ITER < 0 the system is re-solved in FP64 (A overwritten by its LU, ipiv/info from
+//   the FP64 factorisation, X = A^{-1} B).  B is never modified.
+// Stopping rule (LAPACK dsgesv): every column satisfies ||r||_inf <= ||x||_inf * cte with
+// cte = ||A||_inf * eps * sqrt(n), eps = 2^-53.
+//
+// Pipeline (all on the handle's stream, no host synchronisation):
+//   1. convert : A -> FP32 copy in the workspace, ||A||_inf, overflow flags, info = iter = 0
+//   2. sgetrf  : FP32 LU of the copy (same kernels as getrf, FP32 instantiation)
+//   3. refine  : one CTA per matrix: x = LU32^{-1} b, then r = b - A x in FP64 (A read in
+//                FP64), d = LU32^{-1} r in FP32, x += d, until the stopping rule holds
+//   4. fallback: FP64 getrf + getrs gated to the members whose refinement failed.
+#include <math.h>
+
+#include "handle.h"
+#include "launch.h"
+#include "trsv.cuh"
+
+namespace rsb {
+
+constexpr int DSGESV_ITERMAX = 10;
+
+__global__ void __launch_bounds__(256)
+    dsgesv_convert_kernel(int n, Batch<double> A, int lda, float* a32, double* anrm, int* flag,
+                          int* info, int* iter)
+{
+    __shared__ double red[8];
+    __shared__ int ovf;
+    const int64_t b = blockIdx.x;
+    const double* a = A.at(b);
+    float* s = a32 + (size_t)b * n * n;
+    if(threadIdx.x == 0)
+        ovf = 0;
+    __syncthreads();
+    double rmax = 0.0;
+    int ov = 0;
+    for(int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        double rs = 0.0;
+        for(int j = 0; j < n; ++j)
+        {
+            const double v = a[ix(i, j, lda)];
+            ov |= (v > (double)FLT_MAX || v < -(double)FLT_MAX);
+            s[ix(i, j, n)] = (float)v;
+            rs += fabs(v);
+        }
+        rmax = fmax(rmax, rs);
+    }
+    for(int o = 16; o > 0; o >>= 1)
+        rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+    if((threadIdx.x & 31) == 0)
+        red[threadIdx.x >> 5] = rmax;
+    if(ov)
+        atomicOr(&ovf, 1);
+    __syncthreads();
+    if(threadIdx.x == 0)
+    {
+        double m = 0.0;
+        for(int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            m = fmax(m, red[w]);
+        anrm[b] = m;
+        flag[b] = ovf;
+        info[b] = 0;
+        iter[b] = 0;
+    }
+}
+
+// block-wide max of a non-negative value; all threads get the result
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double* red)
+{
+    for(int o = 16; o > 0; o >>= 1)
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if((threadIdx.x & 31) == 0)
+        red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double m = red[0];
+#pragma unroll
+    for(int w = 1; w < NT / 32; ++w)
+        m = fmax(m, red[w]);
+    return m;
+}
+
+template <int NT, int NRC>
+__global__ void __launch_bounds__(NT)
+    dsgesv_refine_kernel(int n, int nrhs, Batch<double> A, int lda, const float* lu32,
+                         const int* ipiv, int64_t strideP, Batch<double> B, int ldb,
+                         Batch<double> X, int ldx, const double* anrm, int* flag,
+                         const int* info32, int* iter, int itermax)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* xs = reinterpret_cast<double*>(smem_raw);   // n x nrhs
+    double* rs = xs + (size_t)n * nrhs;                    // n x nrhs
+    double* red = rs + (size_t)n * nrhs;                   // NT/32
+    float* s32 = reinterpret_cast<float*>(red + NT / 32);  // n x NRC
+    int* perm = reinterpret_cast<int*>(s32 + (size_t)n * NRC);
+    __shared__ int bad;
+
+    const int64_t b = blockIdx.x;
+    const int tid = threadIdx.x;
+    if(flag[b] != 0 || info32[b] != 0)
+    {
+        __syncthreads();
+        if(tid == 0)
+        {
+            iter[b] = flag[b] != 0 ? -2 : -3;
+            flag[b] = 1;
+        }
+        return;
+    }
+    const double* a = A.at(b);
+    const double* bb = B.at(b);
+    double* x = X.at(b);
+    const float* lu = lu32 + (size_t)b * n * n;
+    build_perm(ipiv + b * strideP, n, perm);
+    const double cte = anrm[b] * (DBL_EPSILON * 0.5) * sqrt((double)n);
+    const int tot = n * nrhs;
+    for(int e = tid; e < tot; e += NT)
+    {
+        const int i = e % n, c = e / n;
+        rs[e] = bb[ix(i, c, ldb)];
+        xs[e] = 0.0;
+    }
+    if(tid == 0)
+        bad = 0;
+    __syncthreads();
+    for(int it = 0;; ++it)
+    {
+        // ---- correction d = (LU32)^{-1} P r in FP32, x += d
+        for(int c0 = 0; c0 < nrhs; c0 += NRC)
+        {
+            const int nc = min(NRC, nrhs - c0);
+            for(int e = tid; e < n * nc; e += NT)
+            {
+                const int i = e % n, c = e / n;
+                const double v = rs[perm[i] + (c0 + c) * n];
+                if(v > (double)FLT_MAX || v < -(double)FLT_MAX)
+                    bad = 1;
+                s32[i + c * n] = (float)v;
+            }
+            __syncthreads();
+            block_sweep<float, NT, NRC>(true, true, TriView<float>{lu, 1, n}, n, s32, nc);
+            block_sweep<float, NT, NRC>(false, false, TriView<float>{lu, 1, n}, n, s32, nc);
+            for(int e = tid; e < n * nc; e += NT)
+            {
+                const int i = e % n, c = e / n;
+                xs[i + (c0 + c) * n] += (double)s32[i + c * n];
+            }
+            __syncthreads();
+        }
+        if(bad)
+        {
+            if(tid == 0)
+            {
+                iter[b] = -2;
+                flag[b] = 1;
+            }
+            return;
+        }
+        // ---- residual r = b - A x in FP64 (column-major A: threads over rows coalesce)
+        for(int i = tid; i < n; i += NT)
+        {
+            for(int c = 0; c < nrhs; ++c)
+            {
+                double acc = bb[ix(i, c, ldb)];
+                const double* xc = xs + (size_t)c * n;
+                int j = 0;
+                for(; j + 4 <= n; j += 4)
+                {
+                    const double a0 = a[ix(i, j, lda)], a1 = a[ix(i, j + 1, lda)];
+                    const double a2 = a[ix(i, j + 2, lda)], a3 = a[ix(i, j + 3, lda)];
+                    acc = fma(-a0, xc[j], acc);
+                    acc = fma(-a1, xc[j + 1], acc);
+                    acc = fma(-a2, xc[j + 2], acc);
+                    acc = fma(-a3, xc[j + 3], acc);
+                }
+                for(; j < n; ++j)
+                    acc = fma(-a[ix(i, j, lda)], xc[j], acc);
+                rs[i + c * n] = acc;
+            }
+        }
+        __syncthreads();
+        // ---- stopping rule, every column
+        bool conv = true;
+        for(int c = 0; c < nrhs; ++c)
+        {
+            double xm = 0.0, rm = 0.0;
+            for(int i = tid; i < n; i += NT)
+            {
+                xm = fmax(xm, fabs(xs[i + c * n]));
+                rm = fmax(rm, fabs(rs[i + c * n]));
+            }
+            const double XN = block_max<NT>(xm, red);
+            const double RN = block_max<NT>(rm, red);
+            if(RN > XN * cte)
+                conv = false;
+        }
+        if(conv)
+        {
+            for(int e = tid; e < tot; e += NT)
+            {
+                const int i = e % n, c = e / n;
+                x[ix(i, c, ldx)] = xs[e];
+            }
+            if(tid == 0)
+                iter[b] = it;
+            return;
+        }
+        if(it == itermax)
+        {
+            if(tid == 0)
+            {
+                iter[b] = -(itermax + 1);
+                flag[b] = 1;
+            }
+            return;
+        }
+    }
+}
+
+// X = B for the gated members (the FP64 fallback restarts from B)
+__global__ void copy_gated_kernel(int n, int nrhs, Batch<double> B, int ldb, Batch<double> X,
+                                  int ldx, Gate gate)
+{
+    const int64_t b = blockIdx.x;
+    if(gate.skip(b))
+        return;
+    const double* s = B.at(b);
+    double* d = X.at(b);
+    for(int e = threadIdx.x; e < n * nrhs; e += blockDim.x)
+    {
+        const int i = e % n, c = e / n;
+        d[ix(i, c, ldx)] = s[ix(i, c, ldb)];
+    }
+}
+
+// mark every member for the FP64 path with ITER = -1 (refinement not attempted)
+__global__ void mark_all_kernel(int bc, int* flag, int* info, int* iter)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < bc)
+    {
+        flag[i] = 1;
+        info[i] = 0;
+        iter[i] = -1;
+    }
+}
+
+static size_t refine_smem(int n, int nrhs, int NRC, int NT)
+{
+    return sizeof(double) * (2 * (size_t)n * nrhs + NT / 32) + sizeof(float) * (size_t)n * NRC
+           + sizeof(int) * (size_t)n;
+}
+
+size_t dsgesv_workspace(int n, int nrhs, int bc)
+{
+    (void)nrhs;
+    return ws_round(sizeof(float) * (size_t)n * n * bc) + ws_round(sizeof(double) * bc)
+           + 3 * ws_round(sizeof(int) * bc);
+}
+
+rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, int lda,
+                             int* ipiv, int64_t strideP, Batch<double> B, int ldb,
+                             Batch<double> X, int ldx, int* iter, int* info, int bc, void* ws)
+{
+    char* p = static_cast<char*>(ws);
+    float* a32 = reinterpret_cast<float*>(p);
+    p += ws_round(sizeof(float) * (size_t)n * n * bc);
+    double* anrm = reinterpret_cast<double*>(p);
+    p += ws_round(sizeof(double) * bc);
+    int* flag = reinterpret_cast<int*>(p);
+    p += ws_round(sizeof(int) * bc);
+    int* info32 = reinterpret_cast<int*>(p);
+
+    constexpr int NT = 256;
+    const int NRC = nrhs == 1 ? 1 : 4;
+    const size_t smem = refine_smem(n, nrhs, NRC, NT);
+    const bool refine_ok = smem <= 200 * 1024 && n <= MAX_CTA_ROWS;
+    if(refine_ok)
+    {
+        dsgesv_convert_kernel<<<bc, 256, 0, s>>>(n, A, lda, a32, anrm, flag, info, iter);
+        if(cudaGetLastError() != cudaSuccess)
+            return rocblas_status_internal_error;
+        rocblas_status st = launch_getrf<float>(s, n, n, strided<float>(a32, (int64_t)n * n), n,
+                                                ipiv, strideP, info32, bc, true, Gate{flag, 0});
+        if(st != rocblas_status_success)
+            return st;
+        if(NRC == 1)
+        {
+            auto k = dsgesv_refine_kernel<NT, 1>;
+            if(smem > 48 * 1024
+               && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem)
+                      != cudaSuccess)
+                return rocblas_status_internal_error;
+            k<<<bc, NT, smem, s>>>(n, nrhs, A, lda, a32, ipiv, strideP, B, ldb, X, ldx, anrm, flag,
+                                   info32, iter, DSGESV_ITERMAX);
+        }
+        else
+        {
+            auto k = dsgesv_refine_kernel<NT, 4>;
+            if(smem > 48 * 1024
+               && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem)
+                      != cudaSuccess)
+                return rocblas_status_internal_error;
+            k<<<bc, NT, smem, s>>>(n, nrhs, A, lda, a32, ipiv, strideP, B, ldb, X, ldx, anrm, flag,
+                                   info32, iter, DSGESV_ITERMAX);
+        }
+        if(cudaGetLastError() != cudaSuccess)
+            return rocblas_status_internal_error;
+    }
+    else
+    {
+        mark_all_kernel<<<(bc + 255) / 256, 256, 0, s>>>(bc, flag, info, iter);
+    }
+    // FP64 fallback for the flagged members
+    const Gate g{flag, 1};
+    rocblas_status st = launch_getrf<double>(s, n, n, A, lda, ipiv, strideP, info, bc, true, g);
+    if(st != rocblas_status_success)
+        return st;
+    copy_gated_kernel<<<bc, 256, 0, s>>>(n, nrhs, B, ldb, X, ldx, g);
+    if(cudaGetLastError() != cudaSuccess)
+        return rocblas_status_internal_error;
+    return launch_getrs<double>(s, 0, n, nrhs, A, lda, ipiv, strideP, X, ldx, info, bc, g);
+}
+
+} // namespace rsb

@@ -136,13 +136,51 @@ __device__ __forceinline__ void build_perm(const int* piv, int n, int* perm)
     __syncthreads();
 }
 
+// Solve with getrf factors for all nrhs columns (groups of NRC through shared memory
+// sb[n*NRC] and perm[n]).  Called by all threads of the CTA.
+template <typename T, int NT, int NRC>
+__device__ __forceinline__ void getrs_dev(int trans, int n, int nrhs, const T* a, int lda,
+                                          const int* piv, T* x, int ldb, T* sb, int* perm)
+{
+    if(piv)
+        build_perm(piv, n, perm);
+    for(int c0 = 0; c0 < nrhs; c0 += NRC)
+    {
+        const int nc = min(NRC, nrhs - c0);
+        for(int e = threadIdx.x; e < n * nc; e += NT)
+        {
+            const int i = e % n, c = e / n;
+            const int src = (!trans && piv) ? perm[i] : i;
+            sb[i + c * n] = x[ix(src, c0 + c, ldb)];
+        }
+        __syncthreads();
+        if(!trans)
+        {
+            block_sweep<T, NT, NRC>(true, true, TriView<T>{a, 1, lda}, n, sb, nc);
+            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc);
+        }
+        else
+        {
+            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc);
+            block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sb, nc);
+        }
+        for(int e = threadIdx.x; e < n * nc; e += NT)
+        {
+            const int i = e % n, c = e / n;
+            const int dst = (trans && piv) ? perm[i] : i;
+            x[ix(dst, c0 + c, ldb)] = sb[i + c * n];
+        }
+        __syncthreads();
+    }
+}
+
 // getrs for any n: trans == 0: P b, L (unit) forward, U backward;
 // trans != 0: U' forward, L' (unit) backward, P' x.
 // (library/src/lapack/roclapack_getrs.hpp:117-150)
 template <typename T, int NT, int NRC>
 __global__ void __launch_bounds__(NT)
     getrs_cta_kernel(int trans, int n, int nrhs, Batch<T> A, int lda, const int* ipiv,
-                     int64_t strideP, Batch<T> B, int ldb, const int* skip_info)
+                     int64_t strideP, Batch<T> B, int ldb, const int* skip_info, Gate gate)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sb = reinterpret_cast<T*>(smem_raw);
@@ -151,7 +189,7 @@ __global__ void __launch_bounds__(NT)
     const int64_t b = blockIdx.x / groups;
     const int c0 = (blockIdx.x % groups) * NRC;
     const int nc = min(NRC, nrhs - c0);
-    if(skip_info && skip_info[b] != 0)
+    if((skip_info && skip_info[b] != 0) || gate.skip(b))
         return;
     const T* a = A.at(b);
     T* x = B.at(b);

@@ -34,8 +34,9 @@ def gpu_potrf(handle, A, lower, lda=None, batched=False):
     p = prefix(A.dtype)
     uplo = rs.FILL_LOWER if lower else rs.FILL_UPPER
     if batched:
-        st = rs.call(f"rocsolver_{p}potrf_batched", handle, uplo, n,
-                     ptr(ptr_array(dA, bc, lda * n)), lda, ptr(dI), bc)
+        arr = ptr_array(dA, bc, lda * n)  # keep alive until the kernel has run
+        st = rs.call(f"rocsolver_{p}potrf_batched", handle, uplo, n, ptr(arr), lda, ptr(dI), bc)
+        host(dI)
     else:
         st = rs.call(f"rocsolver_{p}potrf_strided_batched", handle, uplo, n, ptr(dA), lda,
                      lda * n, ptr(dI), bc)
@@ -99,8 +100,10 @@ def gpu_potrs(handle, C, B, lower, batched=False):
     p = prefix(C.dtype)
     uplo = rs.FILL_LOWER if lower else rs.FILL_UPPER
     if batched:
-        st = rs.call(f"rocsolver_{p}potrs_batched", handle, uplo, n, nrhs,
-                     ptr(ptr_array(dA, bc, n * n)), n, ptr(ptr_array(dB, bc, n * nrhs)), n, bc)
+        aA, aB = ptr_array(dA, bc, n * n), ptr_array(dB, bc, n * nrhs)
+        st = rs.call(f"rocsolver_{p}potrs_batched", handle, uplo, n, nrhs, ptr(aA), n, ptr(aB),
+                     n, bc)
+        host(dB)
     else:
         st = rs.call(f"rocsolver_{p}potrs_strided_batched", handle, uplo, n, nrhs, ptr(dA), n,
                      n * n, ptr(dB), n, n * nrhs, bc)

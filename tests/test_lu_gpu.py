@@ -49,6 +49,7 @@ def gpu_getrf(handle, A, lda=None, stride=None, pivot=True, batched=False, strid
         else:
             st = rs.call(f"rocsolver_{p}getrf_npvt_batched", handle, m, n, ptr(arr), lda,
                          ptr(dI), bc)
+        host(dI)
     elif pivot:
         st = rs.call(f"rocsolver_{p}getrf_strided_batched", handle, m, n, ptr(dA), lda, stride,
                      ptr(dP), strideP, ptr(dI), bc)
@@ -197,6 +198,7 @@ def gpu_getrs(handle, trans, LU, ipiv, B, ldb=None, batched=False):
         aB = ptr_array(dB, bc, ldb * nrhs)
         st = rs.call(f"rocsolver_{p}getrs_batched", handle, op, n, nrhs, ptr(aA), n, ptr(dP), n,
                      ptr(aB), ldb, bc)
+        host(dB)
     else:
         st = rs.call(f"rocsolver_{p}getrs_strided_batched", handle, op, n, nrhs, ptr(dA), n,
                      n * n, ptr(dP), n, ptr(dB), ldb, ldb * nrhs, bc)
@@ -248,8 +250,10 @@ def gpu_gesv(handle, A, B, batched=False):
     dI = dev(np.full(bc, -3, np.int32))
     p = prefix(A.dtype)
     if batched:
-        st = rs.call(f"rocsolver_{p}gesv_batched", handle, n, nrhs, ptr(ptr_array(dA, bc, n * n)),
-                     n, ptr(dP), n, ptr(ptr_array(dB, bc, n * nrhs)), n, ptr(dI), bc)
+        aA, aB = ptr_array(dA, bc, n * n), ptr_array(dB, bc, n * nrhs)  # alive until run
+        st = rs.call(f"rocsolver_{p}gesv_batched", handle, n, nrhs, ptr(aA), n, ptr(dP), n,
+                     ptr(aB), n, ptr(dI), bc)
+        host(dI)
     else:
         st = rs.call(f"rocsolver_{p}gesv_strided_batched", handle, n, nrhs, ptr(dA), n, n * n,
                      ptr(dP), n, ptr(dB), n, n * nrhs, ptr(dI), bc)
