@@ -94,9 +94,8 @@ rocblas_status launch_solve_adjoint(cudaStream_t s, int kind, int n, int nrhs, B
     if(smem > 200 * 1024)
         return rocblas_status_not_implemented;
     auto k = solve_adjoint_kernel<T, NT, NRC>;
-    if(smem > 48 * 1024
-       && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-              != cudaSuccess)
+    if(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+       != cudaSuccess)
         return rocblas_status_internal_error;
     k<<<bc, NT, smem, s>>>(kind, n, nrhs, A, lda, ipiv, strideP, X, ldx, G, ldg, GA, ldga, GB,
                            ldgb);

@@ -17,11 +17,11 @@ static inline rocblas_status launch_status()
                                              : rocblas_status_internal_error;
 }
 
+// Opt in to the dynamic shared memory a launch needs (static shared memory of the kernel
+// counts against the same 48 KiB default, so the attribute is always set).
 template <typename K>
 static inline bool set_smem(K kernel, size_t bytes)
 {
-    if(bytes <= 48 * 1024)
-        return true;
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)bytes)
            == cudaSuccess;
@@ -239,7 +239,7 @@ rocblas_status launch_potrf(cudaStream_t s, int upper, int n, Batch<T> A, int ld
     if(n <= 32)
         return run_potrf<T, 32, 1, 32, 8>(s, upper, n, A, lda, info, bc);
     if(n <= 64)
-        return run_potrf<T, 64, 1, 64, 8>(s, upper, n, A, lda, info, bc);
+        return run_potrf<T, 64, 1, 32, 8>(s, upper, n, A, lda, info, bc);
     if(n <= 256)
         return run_potrf<T, 256, 1, 32, 8>(s, upper, n, A, lda, info, bc);
     if(n <= 512)

@@ -296,10 +296,9 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
         if(NRC == 1)
         {
             auto k = dsgesv_refine_kernel<NT, 1>;
-            if(smem > 48 * 1024
-               && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem)
-                      != cudaSuccess)
+            if(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem)
+               != cudaSuccess)
                 return rocblas_status_internal_error;
             k<<<bc, NT, smem, s>>>(n, nrhs, A, lda, a32, ipiv, strideP, B, ldb, X, ldx, anrm, flag,
                                    info32, iter, DSGESV_ITERMAX);
@@ -307,10 +306,9 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
         else
         {
             auto k = dsgesv_refine_kernel<NT, 4>;
-            if(smem > 48 * 1024
-               && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem)
-                      != cudaSuccess)
+            if(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem)
+               != cudaSuccess)
                 return rocblas_status_internal_error;
             k<<<bc, NT, smem, s>>>(n, nrhs, A, lda, a32, ipiv, strideP, B, ldb, X, ldx, anrm, flag,
                                    info32, iter, DSGESV_ITERMAX);

@@ -234,9 +234,8 @@ static rocblas_status run_vb(cudaStream_t s, VbArgs v, T* const* A, T* const* B)
     if(solve > smem)
         smem = solve;
     auto k = vb_persistent_kernel<T, NT, R, JB, TN>;
-    if(smem > 48 * 1024
-       && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-              != cudaSuccess)
+    if(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+       != cudaSuccess)
         return rocblas_status_internal_error;
     int per_sm = 1;
     if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem) != cudaSuccess
