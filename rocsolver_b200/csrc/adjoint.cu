@@ -22,7 +22,8 @@ __global__ void __launch_bounds__(NT)
 {
     // kind: 0 = LU (getrf factors), 1 = Cholesky lower, 2 = Cholesky upper
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* sg = reinterpret_cast<T*>(smem_raw);   // n x NRC  (gB columns of the group)
+    T* sdiag = reinterpret_cast<T*>(smem_raw); // staged diagonal blocks
+    T* sg = sdiag + SDIAG_ELEMS;               // n x NRC  (gB columns of the group)
     T* sx = sg + (size_t)n * NRC;              // n x NRC  (X columns of the group)
     int* perm = reinterpret_cast<int*>(sx + (size_t)n * NRC);
     const int64_t b = blockIdx.x;
@@ -46,18 +47,18 @@ __global__ void __launch_bounds__(NT)
         if(kind == 0)
         {
             // A' y = g  with  A = P' L U  ->  U' L' (P y) = g
-            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sg, nc);
-            block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sg, nc);
+            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
+            block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
         }
         else if(kind == 1)
         {
-            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, 1, lda}, n, sg, nc);
-            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, lda, 1}, n, sg, nc);
+            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, 1, lda}, n, sg, nc, sdiag);
+            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
         }
         else
         {
-            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sg, nc);
-            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sg, nc);
+            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
+            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sg, nc, sdiag);
         }
         // gB (inverse row interchanges for LU: gB[perm[i]] = y[i])
         for(int e = threadIdx.x; e < n * nc; e += NT)
@@ -90,7 +91,7 @@ rocblas_status launch_solve_adjoint(cudaStream_t s, int kind, int n, int nrhs, B
 {
     constexpr int NT = 256;
     constexpr int NRC = 8;
-    const size_t smem = sizeof(T) * 2 * (size_t)n * NRC + sizeof(int) * (size_t)n;
+    const size_t smem = sizeof(T) * (2 * (size_t)n * NRC + SDIAG_ELEMS) + sizeof(int) * (size_t)n;
     if(smem > 200 * 1024)
         return rocblas_status_not_implemented;
     auto k = solve_adjoint_kernel<T, NT, NRC>;

@@ -74,13 +74,13 @@ template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
 static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, int lda,
                                     int* ipiv, int64_t sP, int* info, int bc, Gate g)
 {
-    // U12 chunk width: multiple of TN, at most 64 KiB of shared memory
-    int cw = (int)((64 * 1024) / (sizeof(T) * JB));
-    cw = cw / TN * TN;
-    const int need = ((n + TN - 1) / TN) * TN;
-    if(need < cw)
-        cw = need < TN ? TN : need;
-    const size_t smem = CtaLuSmem<T, NT, JB>::bytes(cw, R);
+    // trailing column chunk: multiple of 32 columns (FP64: 64, FP32: 128 at most), so that
+    // two CTAs fit in an SM's shared memory
+    const int cwmax = sizeof(T) == 8 ? 64 : 128;
+    int cw = ((n + 31) / 32) * 32;
+    if(cw > cwmax)
+        cw = cwmax;
+    const size_t smem = CtaLuSmem<T, NT, JB>::bytes(m, cw, R);
     auto k = getrf_cta_kernel<T, NT, R, JB, TN, PIVOT>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
@@ -153,7 +153,7 @@ static rocblas_status run_getrs_cta(cudaStream_t s, int trans, int n, int nrhs, 
                                     int lda, const int* ipiv, int64_t sP, Batch<T> B, int ldb,
                                     const int* skip, int bc, Gate g)
 {
-    const size_t smem = sizeof(T) * (size_t)n * NRC + sizeof(int) * (size_t)n;
+    const size_t smem = sizeof(T) * ((size_t)n * NRC + SDIAG_ELEMS) + sizeof(int) * (size_t)n;
     auto k = getrs_cta_kernel<T, 256, NRC>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
@@ -255,7 +255,7 @@ template <typename T, int NRC>
 static rocblas_status run_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A,
                                 int lda, Batch<T> B, int ldb, const int* skip, int bc)
 {
-    const size_t smem = sizeof(T) * (size_t)n * NRC;
+    const size_t smem = sizeof(T) * ((size_t)n * NRC + SDIAG_ELEMS);
     auto k = potrs_cta_kernel<T, 256, NRC>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;

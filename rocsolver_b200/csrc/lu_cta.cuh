@@ -5,16 +5,24 @@
 // getrf_panelLU :423-525, getrf_row_permutate :172-210, rocsolver_trsm_lower and the
 // rocBLAS GEMM trailing update :721-732), which issues ~100 launches per call at n=256.
 //
-// B200 design: ONE launch, one CTA per matrix, the whole factorisation in the CTA:
-//   * panel (rows j0..m-1, JB columns) resident in registers, R rows per thread; the
-//     column pivot is a warp redux.sync argmax plus one __syncthreads per column (each
-//     warp publishes its candidate row, so the winner's row is broadcast by the same
-//     barrier); row interchanges inside the panel are lane relabellings;
-//   * the panel's interchanges are applied to the other columns as ONE gather/scatter of
-//     the moved rows (at most 2*JB of them) instead of JB serial swaps;
-//   * U12 = L11^{-1} A12 with one thread per column (L11 broadcast from shared memory);
-//   * A22 -= L21 U12 with the L21 rows still in the registers that factored them and
-//     U12 broadcast from shared memory; A22 is streamed from L2/HBM once per panel.
+// B200 design: ONE launch, one CTA per matrix, the whole factorisation in the CTA.
+//   * Panel (rows j0..m-1, JB columns) in registers, R rows per thread ("slot").  The
+//     column loop is a rolled loop: the active column is always register 0, and the
+//     rank-1 update writes element i+1 into register i, so the shift costs nothing and
+//     the loop body is one copy of the code (no instruction-cache pressure).  The pivot
+//     is a warp redux.sync argmax; each warp publishes its candidate row and the
+//     candidate's reciprocal, so ONE __syncthreads per column broadcasts the winner.
+//     Row interchanges inside the panel are relabellings; finished L entries (negated)
+//     and U rows are parked in shared memory by slot, which is also the A operand of
+//     the trailing update.
+//   * The panel's interchanges reach the other columns as a warp-local gather/scatter of
+//     the moved rows (at most 2*JB) per column: no CTA barrier inside.
+//   * U12 = L11^{-1} A12 as a small GEMM: one warp inverts the unit-lower L11 once per
+//     panel, then warps multiply 32-column tiles in place in shared memory.
+//   * A22 -= L21 U12 as 32x32 warp tiles; A22 is streamed from L2/HBM once per panel.
+//   FP64 tiles run on the FP64 tensor path (mma.sync.m8n8k4.f64, 256 FMAs per instruction;
+//   tcgen05 has no FP64 kind); FP32 tiles are 4x8 register tiles per lane.  Shared-memory
+//   operands have leading dimension = 4 (mod 16) elements (bank-conflict-free fragments).
 #pragma once
 
 #include "common.cuh"
@@ -25,53 +33,179 @@ template <typename T, int NT, int JB>
 struct CtaLuSmem
 {
     static constexpr int NW = NT / 32;
-    // byte offsets inside dynamic shared memory
-    static __host__ __device__ size_t bytes(int cw, int R)
+    static constexpr int LDI = 36;          // L11 inverse, column-major 32 x 32 (+pad)
+    static constexpr int L11LD = 33;        // L11 staging, column-major
+    static __host__ __device__ int ldp(int m) { return ((m + 31) / 32) * 32 + 4; }
+    static __host__ __device__ int cwp(int cw) { return cw + 4; }
+    static __host__ __device__ size_t bytes(int m, int cw, int R)
     {
         using K = typename KeyOf<T>::type;
         size_t s = 0;
-        s += sizeof(T) * JB * JB;       // L11 (column-major, ld JB)
-        s += sizeof(T) * (size_t)JB * cw; // U12 chunk (row-major, ld cw)
-        s += sizeof(T) * 2 * NW * JB;   // candidate rows
-        s += sizeof(K) * 2 * NW;        // candidate keys
-        s += sizeof(int) * 2 * NW;      // candidate rows ids
-        s += sizeof(int) * (size_t)R * NT; // src map
-        s += sizeof(int) * 2 * JB;      // moved list
-        s += sizeof(int) * (JB + 2);    // panel pivots, counter
+        s += sizeof(T) * (size_t)JB * ldp(m);   // panel slots: -L (and U rows), [k][slot]
+        s += sizeof(T) * (size_t)JB * cwp(cw);  // A12 / U12 chunk, [k][col]
+        s += sizeof(T) * 32 * LDI;              // L11^{-1}
+        s += sizeof(T) * 32 * L11LD;            // L11
+        s += sizeof(T) * 2 * NW * JB;           // candidate rows
+        s += sizeof(T) * 2 * NW;                // candidate reciprocals
+        s += sizeof(K) * 2 * NW;                // candidate keys
+        s += sizeof(int) * 2 * NW;              // candidate positions
+        s += sizeof(int) * (size_t)R * NT;      // slot of each position
+        s += sizeof(int) * 4 * JB;              // moved positions and their sources
+        s += sizeof(int) * (JB + 2);            // panel pivots, counter
         return (s + 15) & ~size_t(15);
     }
 };
 
-// Factor one m x n matrix with the whole CTA.  smem_raw must hold CtaLuSmem::bytes(cw, R);
-// m <= R*NT.  Writes ipiv (1-based, PIVOT only) and *info_out.  Called by all threads.
+// ---------------------------------------------------------------------------------------
+// Warp tile products.  acc (32 x 32 tile) += A * B over k < K where A(r, k) = sA[k*lda_s +
+// arow] (arow: this lane's fragment rows, identity or through the slot table) and
+// B(k, c) = sB[k*ldb_s + c0 + c].
+template <typename T>
+struct WarpTile;
+
+template <>
+struct WarpTile<double>
+{
+    double acc[4][4][2];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for(int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for(int ni = 0; ni < 4; ++ni)
+                acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+    }
+    template <int K>
+    __device__ __forceinline__ void mma(const double* sA, int lda_s, const int (&arow)[4],
+                                        const double* sB, int ldb_s, int c0)
+    {
+        const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+#pragma unroll 2
+        for(int k0 = 0; k0 < K; k0 += 4)
+        {
+            double af[4], bf[4];
+#pragma unroll
+            for(int mi = 0; mi < 4; ++mi)
+                af[mi] = sA[(k0 + tq) * lda_s + arow[mi]];
+#pragma unroll
+            for(int ni = 0; ni < 4; ++ni)
+                bf[ni] = sB[(k0 + tq) * ldb_s + c0 + ni * 8 + g];
+#pragma unroll
+            for(int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for(int ni = 0; ni < 4; ++ni)
+                    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 "
+                                 "{%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                                 : "+d"(acc[mi][ni][0]), "+d"(acc[mi][ni][1])
+                                 : "d"(af[mi]), "d"(bf[ni]));
+        }
+    }
+    // visit every tile element this lane holds: f(row in tile, col in tile, value&)
+    template <typename F>
+    __device__ __forceinline__ void each(F f)
+    {
+        const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+#pragma unroll
+        for(int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for(int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for(int e = 0; e < 2; ++e)
+                    f(mi * 8 + g, ni * 8 + tq * 2 + e, acc[mi][ni][e]);
+    }
+    static __device__ __forceinline__ int frag_row(int mi)
+    {
+        return mi * 8 + ((threadIdx.x & 31) >> 2);
+    }
+};
+
+template <>
+struct WarpTile<float>
+{
+    float acc[4][8];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for(int i = 0; i < 4; ++i)
+#pragma unroll
+            for(int j = 0; j < 8; ++j)
+                acc[i][j] = 0.f;
+    }
+    template <int K>
+    __device__ __forceinline__ void mma(const float* sA, int lda_s, const int (&arow)[4],
+                                        const float* sB, int ldb_s, int c0)
+    {
+        const int cg = (threadIdx.x & 31) >> 3;
+#pragma unroll 4
+        for(int k = 0; k < K; ++k)
+        {
+            float lv[4];
+#pragma unroll
+            for(int i = 0; i < 4; ++i)
+                lv[i] = sA[k * lda_s + arow[i]];
+            const float4 u0 = *reinterpret_cast<const float4*>(sB + k * ldb_s + c0 + cg * 8);
+            const float4 u1 = *reinterpret_cast<const float4*>(sB + k * ldb_s + c0 + cg * 8 + 4);
+            const float uv[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+#pragma unroll
+            for(int i = 0; i < 4; ++i)
+#pragma unroll
+                for(int j = 0; j < 8; ++j)
+                    acc[i][j] = fmaf(lv[i], uv[j], acc[i][j]);
+        }
+    }
+    template <typename F>
+    __device__ __forceinline__ void each(F f)
+    {
+        const int lane = threadIdx.x & 31, rg = lane & 7, cg = lane >> 3;
+#pragma unroll
+        for(int i = 0; i < 4; ++i)
+#pragma unroll
+            for(int j = 0; j < 8; ++j)
+                f(rg * 4 + i, cg * 8 + j, acc[i][j]);
+    }
+    static __device__ __forceinline__ int frag_row(int i)
+    {
+        return ((threadIdx.x & 31) & 7) * 4 + i;
+    }
+};
+
+// Factor one m x n matrix with the whole CTA.  smem_raw must hold CtaLuSmem::bytes(m, cw, R);
+// m <= R*NT; cw is a multiple of 32.  Writes ipiv (1-based, PIVOT only) and *info_out.
+// Called by all threads of the CTA.
 template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
 __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* piv_out,
                                               int* info_out, int cw, unsigned char* smem_raw)
 {
+    static_assert(JB % 4 == 0 && JB <= 32, "panel width");
     using K = typename KeyOf<T>::type;
+    using SM = CtaLuSmem<T, NT, JB>;
     constexpr int NW = NT / 32;
-    T* sL11 = reinterpret_cast<T*>(smem_raw);
-    T* sU = sL11 + JB * JB;
-    T* cand = sU + (size_t)JB * cw; // [2][NW][JB]
-    K* ckey = reinterpret_cast<K*>(cand + 2 * NW * JB);
-    int* crow = reinterpret_cast<int*>(ckey + 2 * NW);
-    int* srcmap = crow + 2 * NW;
-    int* moved = srcmap + R * NT;
-    int* spiv = moved + 2 * JB;
+    const int ldp = SM::ldp(m), cwp = SM::cwp(cw);
+    T* sP = reinterpret_cast<T*>(smem_raw);          // [JB][ldp]
+    T* sU = sP + (size_t)JB * ldp;                     // [JB][cwp]
+    T* sLi = sU + (size_t)JB * cwp;                    // [32][LDI]
+    T* sL11 = sLi + 32 * SM::LDI;                      // [32][L11LD]
+    T* cand = sL11 + 32 * SM::L11LD;                   // [2][NW][JB]
+    T* crcp = cand + 2 * NW * JB;                      // [2][NW]
+    K* ckey = reinterpret_cast<K*>(crcp + 2 * NW);     // [2][NW]
+    int* crow = reinterpret_cast<int*>(ckey + 2 * NW); // [2][NW]
+    int* slotof = crow + 2 * NW;                       // [R*NT]
+    int* moved = slotof + R * NT;                      // [2*JB]
+    int* movsrc = moved + 2 * JB;                      // [2*JB]
+    int* spiv = movsrc + 2 * JB;                       // [JB]
     int* nmoved = spiv + JB;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mn = min(m, n);
     int inf = 0;
 
-    T pv[R][JB];
-    int lrow[R];
-
     for(int j0 = 0; j0 < mn; j0 += JB)
     {
         const int jb = min(JB, mn - j0);
         const int mp = m - j0;
-        // ---- load the panel (rows j0..m-1, columns j0..j0+jb-1)
+        T pv[R][JB];
+        int lrow[R];
+        // ---------------- load the panel (rows j0..m-1, columns j0..j0+jb-1)
 #pragma unroll
         for(int q = 0; q < R; ++q)
         {
@@ -81,257 +215,281 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             for(int c = 0; c < JB; ++c)
                 pv[q][c] = (r < mp && c < jb) ? a[ix(j0 + r, j0 + c, lda)] : T(0);
         }
-        // ---- factor the panel, one barrier per column
-#pragma unroll
-        for(int c = 0; c < JB; ++c)
+        // ---------------- factor the panel: rolled column loop, one barrier per column
+#pragma unroll 1
+        for(int c = 0; c < jb; ++c)
         {
-            if(c < jb)
+            const int buf = c & 1;
+            T* cb = cand + buf * NW * JB;
+            int prow = c, gw = 0;
+            if(PIVOT)
             {
-                const int buf = c & 1;
-                T* cb = cand + (size_t)buf * NW * JB;
-                int prow = c, gw = 0;
-                if(PIVOT)
-                {
-                    K bk = 0;
-                    int br = INT_MAX;
-                    bool any = false;
-#pragma unroll
-                    for(int q = 0; q < R; ++q)
-                    {
-                        const int r = tid + q * NT;
-                        if(r < mp && lrow[q] >= c)
-                        {
-                            K kq = pivot_key(pv[q][c], lrow[q] == c);
-                            if(!any || kq > bk || (kq == bk && lrow[q] < br))
-                            {
-                                bk = kq;
-                                br = lrow[q];
-                                any = true;
-                            }
-                        }
-                    }
-                    K wk;
-                    const int wr = warp_argmax(bk, br, any, &wk);
-                    if(any && br == wr)
-                    {
-#pragma unroll
-                        for(int q = 0; q < R; ++q)
-                            if(lrow[q] == wr && tid + q * NT < mp)
-                            {
-#pragma unroll
-                                for(int cc = 0; cc < JB; ++cc)
-                                    if(cc >= c)
-                                        cb[warp * JB + cc] = pv[q][cc];
-                            }
-                    }
-                    if(lane == 0)
-                    {
-                        ckey[buf * NW + warp] = wk;
-                        crow[buf * NW + warp] = wr;
-                    }
-                    __syncthreads();
-                    K gk = 0;
-                    int gr = INT_MAX;
-                    gw = -1;
-#pragma unroll
-                    for(int w = 0; w < NW; ++w)
-                    {
-                        const int rr = crow[buf * NW + w];
-                        const K kw = ckey[buf * NW + w];
-                        if(rr != INT_MAX && (gw < 0 || kw > gk || (kw == gk && rr < gr)))
-                        {
-                            gk = kw;
-                            gr = rr;
-                            gw = w;
-                        }
-                    }
-                    prow = gr;
-                }
-                else
-                {
-#pragma unroll
-                    for(int q = 0; q < R; ++q)
-                        if(lrow[q] == c && tid + q * NT < mp)
-                        {
-#pragma unroll
-                            for(int cc = 0; cc < JB; ++cc)
-                                if(cc >= c)
-                                    cb[cc] = pv[q][cc];
-                        }
-                    __syncthreads();
-                }
-                const T* prowv = cb + gw * JB;
-                const T pivv = prowv[c];
-                if(tid == 0)
-                    spiv[c] = prow;
-                if(pivv == T(0) && inf == 0)
-                    inf = j0 + c + 1;
-                Scaler<T> s;
-                s.init(pivv);
+                K bk = 0;
+                int br = INT_MAX;
+                bool any = false;
 #pragma unroll
                 for(int q = 0; q < R; ++q)
                 {
-                    if(PIVOT)
+                    if(tid + q * NT < mp && lrow[q] >= c)
                     {
-                        if(lrow[q] == prow)
-                            lrow[q] = c;
-                        else if(lrow[q] == c)
-                            lrow[q] = prow;
+                        const K kq = pivot_key(pv[q][0], lrow[q] == c);
+                        if(!any || kq > bk || (kq == bk && lrow[q] < br))
+                        {
+                            bk = kq;
+                            br = lrow[q];
+                            any = true;
+                        }
                     }
-                    if(tid + q * NT < mp && lrow[q] > c)
-                    {
-                        const T l = s.apply(pv[q][c]);
-                        pv[q][c] = l;
+                }
+                K wk;
+                const int wr = warp_argmax(bk, br, any, &wk);
+                if(any && br == wr)
+                {
 #pragma unroll
-                        for(int cc = 0; cc < JB; ++cc)
-                            if(cc > c)
-                                pv[q][cc] = fma(-l, prowv[cc], pv[q][cc]);
+                    for(int q = 0; q < R; ++q)
+                        if(lrow[q] == wr && tid + q * NT < mp)
+                        {
+#pragma unroll
+                            for(int i = 0; i < JB; ++i)
+                                cb[warp * JB + i] = pv[q][i];
+                            const T p = pv[q][0];
+                            crcp[buf * NW + warp] = p != T(0) ? T(1) / p : T(0);
+                        }
+                }
+                if(lane == 0)
+                {
+                    ckey[buf * NW + warp] = wk;
+                    crow[buf * NW + warp] = wr;
+                }
+                __syncthreads();
+                K gk = 0;
+                int gr = INT_MAX;
+                gw = -1;
+#pragma unroll
+                for(int w = 0; w < NW; ++w)
+                {
+                    const int rr = crow[buf * NW + w];
+                    const K kw = ckey[buf * NW + w];
+                    if(rr != INT_MAX && (gw < 0 || kw > gk || (kw == gk && rr < gr)))
+                    {
+                        gk = kw;
+                        gr = rr;
+                        gw = w;
+                    }
+                }
+                prow = gr;
+            }
+            else
+            {
+#pragma unroll
+                for(int q = 0; q < R; ++q)
+                    if(lrow[q] == c && tid + q * NT < mp)
+                    {
+#pragma unroll
+                        for(int i = 0; i < JB; ++i)
+                            cb[i] = pv[q][i];
+                        const T p = pv[q][0];
+                        crcp[buf * NW] = p != T(0) ? T(1) / p : T(0);
+                    }
+                __syncthreads();
+            }
+            const T* prowv = cb + gw * JB;
+            const T pivv = prowv[0];
+            const T rcp = crcp[buf * NW + gw];
+            if(tid == 0)
+                spiv[c] = prow;
+            if(pivv == T(0) && inf == 0)
+                inf = j0 + c + 1;
+            // LAPACK getf2 scaling: reciprocal when |pivot| >= sfmin, else division
+            const int mode = pivv == T(0) ? 0 : (fabs(pivv) >= Lim<T>::sfmin() ? 1 : 2);
+#pragma unroll
+            for(int q = 0; q < R; ++q)
+            {
+                if(PIVOT)
+                {
+                    if(lrow[q] == prow)
+                        lrow[q] = c;
+                    else if(lrow[q] == c)
+                        lrow[q] = prow;
+                }
+                const int slot = tid + q * NT;
+                if(slot < mp)
+                {
+                    if(lrow[q] == c)
+                    {
+                        // the pivot row: its remaining panel entries are row c of U
+#pragma unroll
+                        for(int i = 0; i < JB; ++i)
+                            if(c + i < jb)
+                                sP[(c + i) * ldp + slot] = pv[q][i];
+                    }
+                    else if(lrow[q] > c)
+                    {
+                        const T x = pv[q][0];
+                        const T l = mode == 1 ? x * rcp : (mode == 2 ? x / pivv : x);
+                        sP[c * ldp + slot] = -l;
+#pragma unroll
+                        for(int i = 0; i + 1 < JB; ++i)
+                            pv[q][i] = fma(-l, prowv[i + 1], pv[q][i + 1]);
                     }
                 }
             }
         }
-        // ---- write the panel back at its final row positions; L11 to shared memory
+        __syncthreads();
+        // ---------------- panel write-back at final positions; slot table; L11
 #pragma unroll
         for(int q = 0; q < R; ++q)
         {
-            const int r = tid + q * NT;
-            if(r < mp)
+            const int slot = tid + q * NT;
+            if(slot < mp)
             {
-#pragma unroll
-                for(int cc = 0; cc < JB; ++cc)
-                    if(cc < jb)
-                        a[ix(j0 + lrow[q], j0 + cc, lda)] = pv[q][cc];
-                if(lrow[q] < jb)
+                const int pos = lrow[q];
+#pragma unroll 4
+                for(int k = 0; k < jb; ++k)
                 {
-#pragma unroll
-                    for(int cc = 0; cc < JB; ++cc)
-                        sL11[cc * JB + lrow[q]] = pv[q][cc];
+                    const T v = sP[k * ldp + slot];
+                    a[ix(j0 + pos, j0 + k, lda)] = k < pos ? -v : v;
                 }
-                srcmap[lrow[q]] = r;
+                slotof[pos] = slot;
             }
         }
         if(tid == 0)
             *nmoved = 0;
         __syncthreads();
+        for(int e = tid; e < 32 * 32; e += NT)
+        {
+            const int i = e & 31, k = e >> 5; // L11(i, k), unit lower
+            T v = T(0);
+            if(i < jb && k < jb)
+                v = i > k ? -sP[k * ldp + slotof[i]] : (i == k ? T(1) : T(0));
+            sL11[k * SM::L11LD + i] = v;
+        }
         if(PIVOT)
         {
             if(tid < jb)
                 piv_out[j0 + tid] = j0 + spiv[tid] + 1;
-            // ---- list of moved rows (positions whose content changed)
             for(int p = tid; p < mp; p += NT)
-                if(srcmap[p] != p)
-                    moved[atomicAdd(nmoved, 1)] = p;
-            __syncthreads();
-            const int nm = *nmoved;
-            // ---- apply the interchanges to the columns outside the panel, whole columns
-            // per round so that no round reads a row a previous round already overwrote
-            const int nother = n - jb;
-            if(nm > 0 && nother > 0)
             {
-                constexpr int KV = 8;
-                const int cols_per_round = max(1, (NT * KV) / nm);
-                for(int cb0 = 0; cb0 < nother; cb0 += cols_per_round)
+                const int s = slotof[p];
+                if(s != p)
                 {
-                    const int ncr = min(cols_per_round, nother - cb0);
-                    const int npairs = ncr * nm;
-                    T val[KV];
-#pragma unroll
-                    for(int v = 0; v < KV; ++v)
-                    {
-                        const int p = tid + v * NT;
-                        if(p < npairs)
-                        {
-                            const int oc = cb0 + p / nm;
-                            const int col = oc < j0 ? oc : oc + jb;
-                            val[v] = a[ix(j0 + srcmap[moved[p % nm]], col, lda)];
-                        }
-                    }
-                    __syncthreads();
-#pragma unroll
-                    for(int v = 0; v < KV; ++v)
-                    {
-                        const int p = tid + v * NT;
-                        if(p < npairs)
-                        {
-                            const int oc = cb0 + p / nm;
-                            const int col = oc < j0 ? oc : oc + jb;
-                            a[ix(j0 + moved[p % nm], col, lda)] = val[v];
-                        }
-                    }
-                    __syncthreads();
+                    const int idx = atomicAdd(nmoved, 1);
+                    moved[idx] = p;
+                    movsrc[idx] = s;
                 }
             }
         }
-        // ---- trailing update, column chunk by column chunk
+        __syncthreads();
+        // ---------------- L11^{-1}: lane j solves L11 x = e_j (column j of the inverse)
+        if(warp == 0)
+        {
+            T x[32];
+#pragma unroll
+            for(int i = 0; i < 32; ++i)
+                x[i] = (i == lane && lane < jb) ? T(1) : T(0);
+#pragma unroll
+            for(int k = 0; k < 32; ++k)
+#pragma unroll
+                for(int i = k + 1; i < 32; ++i)
+                    x[i] = fma(-sL11[k * SM::L11LD + i], x[k], x[i]);
+#pragma unroll
+            for(int i = 0; i < 32; ++i)
+                sLi[lane * SM::LDI + i] = x[i];
+        }
+        // ---------------- row interchanges on the other columns: warp-local per column
+        const int nm = PIVOT ? *nmoved : 0;
+        const int nother = n - jb;
+        if(nm > 0)
+        {
+            for(int o0 = warp * 4; o0 < nother; o0 += NW * 4)
+            {
+                T v[4][2];
+#pragma unroll
+                for(int u = 0; u < 4; ++u)
+                {
+                    const int o = o0 + u;
+                    const int col = o < j0 ? o : o + jb;
+#pragma unroll
+                    for(int s = 0; s < 2; ++s)
+                    {
+                        const int i = lane + 32 * s;
+                        if(o < nother && i < nm)
+                            v[u][s] = a[ix(j0 + movsrc[i], col, lda)];
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for(int u = 0; u < 4; ++u)
+                {
+                    const int o = o0 + u;
+                    const int col = o < j0 ? o : o + jb;
+#pragma unroll
+                    for(int s = 0; s < 2; ++s)
+                    {
+                        const int i = lane + 32 * s;
+                        if(o < nother && i < nm)
+                            a[ix(j0 + moved[i], col, lda)] = v[u][s];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // ---------------- trailing update, column chunk by column chunk
+        const int mt = mp - jb;
         for(int c0 = j0 + jb; c0 < n; c0 += cw)
         {
             const int ncol = min(cw, n - c0);
-            // U12 = L11^{-1} A12: one thread per column (reference dtrsm order L,L,N,U)
-            for(int col = tid; col < ncol; col += NT)
+            const int ncp = (ncol + 31) & ~31;
+            // stage A12 (rows j0..j0+jb-1 of the chunk), zero padded to JB x ncp
+            for(int e = tid; e < JB * ncp; e += NT)
             {
-                T u[JB];
-#pragma unroll
-                for(int k = 0; k < JB; ++k)
-                    u[k] = k < jb ? a[ix(j0 + k, c0 + col, lda)] : T(0);
-#pragma unroll
-                for(int k = 0; k < JB; ++k)
-                {
-#pragma unroll
-                    for(int i = 0; i < JB; ++i)
-                        if(i > k && i < jb)
-                            u[i] = fma(-sL11[k * JB + i], u[k], u[i]);
-                }
-#pragma unroll
-                for(int k = 0; k < JB; ++k)
-                    if(k < jb)
-                    {
-                        a[ix(j0 + k, c0 + col, lda)] = u[k];
-                        sU[(size_t)k * cw + col] = u[k];
-                    }
+                const int k = e % JB, col = e / JB;
+                sU[k * cwp + col] = (k < jb && col < ncol) ? a[ix(j0 + k, c0 + col, lda)] : T(0);
             }
             __syncthreads();
-            // A22 -= L21 * U12 for this chunk; each thread updates its own L21 rows
-            for(int t0 = 0; t0 < ncol; t0 += TN)
+            // U12 = L11^{-1} A12 in place, one 32-column tile per warp
+            for(int t = warp; t < ncp / 32; t += NW)
             {
-                T acc[R][TN];
+                WarpTile<T> w;
+                w.zero();
+                int arow[4];
 #pragma unroll
-                for(int q = 0; q < R; ++q)
+                for(int mi = 0; mi < 4; ++mi)
+                    arow[mi] = WarpTile<T>::frag_row(mi);
+                w.template mma<JB>(sLi, SM::LDI, arow, sU, cwp, t * 32);
+                __syncwarp();
+                w.each([&](int rr, int cc, T& v) {
+                    const int col = t * 32 + cc;
+                    if(rr < JB)
+                        sU[rr * cwp + col] = rr < jb ? v : T(0);
+                    if(rr < jb && col < ncol)
+                        a[ix(j0 + rr, c0 + col, lda)] = v;
+                });
+            }
+            __syncthreads();
+            // A22 -= L21 U12: 32x32 tiles of (mt x ncol); A rows through the slot table
+            const int tm = (mt + 31) / 32, tn = ncp / 32;
+            for(int t = warp; t < tm * tn; t += NW)
+            {
+                const int r0 = (t % tm) * 32, cc0 = (t / tm) * 32;
+                WarpTile<T> w;
+                int arow[4];
+#pragma unroll
+                for(int mi = 0; mi < 4; ++mi)
                 {
-                    const bool mine = (tid + q * NT < mp) && lrow[q] >= jb;
-#pragma unroll
-                    for(int t = 0; t < TN; ++t)
-                        acc[q][t] = (mine && t0 + t < ncol)
-                                        ? a[ix(j0 + lrow[q], c0 + t0 + t, lda)]
-                                        : T(0);
+                    const int r = r0 + WarpTile<T>::frag_row(mi);
+                    arow[mi] = r < mt ? slotof[jb + r] : 0;
                 }
-#pragma unroll
-                for(int k = 0; k < JB; ++k)
-                {
-                    if(k < jb)
-                    {
-                        T uk[TN];
-#pragma unroll
-                        for(int t = 0; t < TN; ++t)
-                            uk[t] = sU[(size_t)k * cw + t0 + t];
-#pragma unroll
-                        for(int q = 0; q < R; ++q)
-#pragma unroll
-                            for(int t = 0; t < TN; ++t)
-                                acc[q][t] = fma(-pv[q][k], uk[t], acc[q][t]);
-                    }
-                }
-#pragma unroll
-                for(int q = 0; q < R; ++q)
-                {
-                    const bool mine = (tid + q * NT < mp) && lrow[q] >= jb;
-                    if(mine)
-                    {
-#pragma unroll
-                        for(int t = 0; t < TN; ++t)
-                            if(t0 + t < ncol)
-                                a[ix(j0 + lrow[q], c0 + t0 + t, lda)] = acc[q][t];
-                    }
-                }
+                w.each([&](int rr, int cc, T& v) {
+                    const int r = r0 + rr, col = cc0 + cc;
+                    v = (r < mt && col < ncol) ? a[ix(j0 + jb + r, c0 + col, lda)] : T(0);
+                });
+                w.template mma<JB>(sP, ldp, arow, sU, cwp, cc0);
+                w.each([&](int rr, int cc, T& v) {
+                    const int r = r0 + rr, col = cc0 + cc;
+                    if(r < mt && col < ncol)
+                        a[ix(j0 + jb + r, c0 + col, lda)] = v;
+                });
             }
             __syncthreads();
         }
@@ -341,7 +499,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
 }
 
 template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 2)
     getrf_cta_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
                      int cw, Gate gate)
 {

@@ -100,7 +100,8 @@ __global__ void __launch_bounds__(NT)
     double* xs = reinterpret_cast<double*>(smem_raw);   // n x nrhs
     double* rs = xs + (size_t)n * nrhs;                    // n x nrhs
     double* red = rs + (size_t)n * nrhs;                   // NT/32
-    float* s32 = reinterpret_cast<float*>(red + NT / 32);  // n x NRC
+    float* sdiag = reinterpret_cast<float*>(red + NT / 32); // staged diagonal blocks
+    float* s32 = sdiag + SDIAG_ELEMS;                       // n x NRC
     int* perm = reinterpret_cast<int*>(s32 + (size_t)n * NRC);
     __shared__ int bad;
 
@@ -147,8 +148,8 @@ __global__ void __launch_bounds__(NT)
                 s32[i + c * n] = (float)v;
             }
             __syncthreads();
-            block_sweep<float, NT, NRC>(true, true, TriView<float>{lu, 1, n}, n, s32, nc);
-            block_sweep<float, NT, NRC>(false, false, TriView<float>{lu, 1, n}, n, s32, nc);
+            block_sweep<float, NT, NRC>(true, true, TriView<float>{lu, 1, n}, n, s32, nc, sdiag);
+            block_sweep<float, NT, NRC>(false, false, TriView<float>{lu, 1, n}, n, s32, nc, sdiag);
             for(int e = tid; e < n * nc; e += NT)
             {
                 const int i = e % n, c = e / n;
@@ -256,8 +257,8 @@ __global__ void mark_all_kernel(int bc, int* flag, int* info, int* iter)
 
 static size_t refine_smem(int n, int nrhs, int NRC, int NT)
 {
-    return sizeof(double) * (2 * (size_t)n * nrhs + NT / 32) + sizeof(float) * (size_t)n * NRC
-           + sizeof(int) * (size_t)n;
+    return sizeof(double) * (2 * (size_t)n * nrhs + NT / 32)
+           + sizeof(float) * ((size_t)n * NRC + SDIAG_ELEMS) + sizeof(int) * (size_t)n;
 }
 
 size_t dsgesv_workspace(int n, int nrhs, int bc)

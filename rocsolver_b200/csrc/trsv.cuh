@@ -29,11 +29,18 @@ struct TriView
     }
 };
 
+constexpr int SDIAG_LD = 33;               // staged diagonal block, padded
+constexpr int SDIAG_ELEMS = 32 * SDIAG_LD;
+
 // Solve M x = b in place for the nc columns of sb (ld = n).  forward: M lower
 // (substitution top-down), else M upper (bottom-up).  unit: unit diagonal.
-// Must be called by all NT threads of the CTA.
+// sdiag: shared scratch of SDIAG_ELEMS elements.  Must be called by all NT threads.
+// Per 32-wide block: all threads stage the diagonal block in shared memory (coalesced
+// along the operand's contiguous direction), warp 0 solves it with shuffles, then all
+// threads apply it to the remaining rows with independent (unrolled) factor loads.
 template <typename T, int NT, int NRC>
-__device__ void block_sweep(bool forward, bool unit, TriView<T> M, int n, T* sb, int nc)
+__device__ void block_sweep(bool forward, bool unit, TriView<T> M, int n, T* sb, int nc,
+                            T* sdiag)
 {
     const unsigned full = 0xffffffffu;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -42,6 +49,22 @@ __device__ void block_sweep(bool forward, bool unit, TriView<T> M, int n, T* sb,
     {
         const int kb = forward ? bi * 32 : (nblk - 1 - bi) * 32;
         const int nb = min(32, n - kb);
+        for(int e = tid; e < nb * nb; e += NT)
+        {
+            int r, c;
+            if(M.rs == 1)
+            {
+                r = e % nb;
+                c = e / nb;
+            }
+            else
+            {
+                c = e % nb;
+                r = e / nb;
+            }
+            sdiag[c * SDIAG_LD + r] = M(kb + r, kb + c);
+        }
+        __syncthreads();
         if(warp == 0)
         {
             T x[NRC];
@@ -52,8 +75,8 @@ __device__ void block_sweep(bool forward, bool unit, TriView<T> M, int n, T* sb,
             {
                 for(int k = 0; k < nb; ++k)
                 {
-                    const T mlk = lane > k && lane < nb ? M(kb + lane, kb + k) : T(0);
-                    const T dkk = unit ? T(1) : M(kb + k, kb + k);
+                    const T mlk = sdiag[k * SDIAG_LD + lane];
+                    const T dkk = unit ? T(1) : sdiag[k * SDIAG_LD + k];
 #pragma unroll
                     for(int c = 0; c < NRC; ++c)
                     {
@@ -69,8 +92,8 @@ __device__ void block_sweep(bool forward, bool unit, TriView<T> M, int n, T* sb,
             {
                 for(int k = nb - 1; k >= 0; --k)
                 {
-                    const T mlk = lane < k ? M(kb + lane, kb + k) : T(0);
-                    const T dkk = unit ? T(1) : M(kb + k, kb + k);
+                    const T mlk = sdiag[k * SDIAG_LD + lane];
+                    const T dkk = unit ? T(1) : sdiag[k * SDIAG_LD + k];
 #pragma unroll
                     for(int c = 0; c < NRC; ++c)
                     {
@@ -97,12 +120,27 @@ __device__ void block_sweep(bool forward, bool unit, TriView<T> M, int n, T* sb,
 #pragma unroll
             for(int c = 0; c < NRC; ++c)
                 acc[c] = c < nc ? sb[i + c * n] : T(0);
-            for(int k = 0; k < nb; ++k)
+            if(nb == 32)
             {
-                const T mik = M(i, kb + k);
+                T mv[32];
 #pragma unroll
-                for(int c = 0; c < NRC; ++c)
-                    acc[c] = fma(-mik, sb[kb + k + c * n], acc[c]);
+                for(int k = 0; k < 32; ++k)
+                    mv[k] = M(i, kb + k);
+#pragma unroll
+                for(int k = 0; k < 32; ++k)
+#pragma unroll
+                    for(int c = 0; c < NRC; ++c)
+                        acc[c] = fma(-mv[k], sb[kb + k + c * n], acc[c]);
+            }
+            else
+            {
+                for(int k = 0; k < nb; ++k)
+                {
+                    const T mik = M(i, kb + k);
+#pragma unroll
+                    for(int c = 0; c < NRC; ++c)
+                        acc[c] = fma(-mik, sb[kb + k + c * n], acc[c]);
+                }
             }
 #pragma unroll
             for(int c = 0; c < NRC; ++c)
@@ -140,7 +178,8 @@ __device__ __forceinline__ void build_perm(const int* piv, int n, int* perm)
 // sb[n*NRC] and perm[n]).  Called by all threads of the CTA.
 template <typename T, int NT, int NRC>
 __device__ __forceinline__ void getrs_dev(int trans, int n, int nrhs, const T* a, int lda,
-                                          const int* piv, T* x, int ldb, T* sb, int* perm)
+                                          const int* piv, T* x, int ldb, T* sb, int* perm,
+                                          T* sdiag)
 {
     if(piv)
         build_perm(piv, n, perm);
@@ -156,13 +195,13 @@ __device__ __forceinline__ void getrs_dev(int trans, int n, int nrhs, const T* a
         __syncthreads();
         if(!trans)
         {
-            block_sweep<T, NT, NRC>(true, true, TriView<T>{a, 1, lda}, n, sb, nc);
-            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc);
+            block_sweep<T, NT, NRC>(true, true, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
+            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
         }
         else
         {
-            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc);
-            block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sb, nc);
+            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
+            block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
         }
         for(int e = threadIdx.x; e < n * nc; e += NT)
         {
@@ -183,7 +222,8 @@ __global__ void __launch_bounds__(NT)
                      int64_t strideP, Batch<T> B, int ldb, const int* skip_info, Gate gate)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* sb = reinterpret_cast<T*>(smem_raw);
+    T* sdiag = reinterpret_cast<T*>(smem_raw);
+    T* sb = sdiag + SDIAG_ELEMS;
     int* perm = reinterpret_cast<int*>(sb + (size_t)n * NRC);
     const int groups = (nrhs + NRC - 1) / NRC;
     const int64_t b = blockIdx.x / groups;
@@ -205,13 +245,13 @@ __global__ void __launch_bounds__(NT)
     __syncthreads();
     if(!trans)
     {
-        block_sweep<T, NT, NRC>(true, true, TriView<T>{a, 1, lda}, n, sb, nc);
-        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc);
+        block_sweep<T, NT, NRC>(true, true, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
     }
     else
     {
-        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc);
-        block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sb, nc);
+        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
     }
     for(int e = threadIdx.x; e < n * nc; e += NT)
     {
@@ -229,7 +269,8 @@ __global__ void __launch_bounds__(NT)
                      const int* skip_info)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* sb = reinterpret_cast<T*>(smem_raw);
+    T* sdiag = reinterpret_cast<T*>(smem_raw);
+    T* sb = sdiag + SDIAG_ELEMS;
     const int groups = (nrhs + NRC - 1) / NRC;
     const int64_t b = blockIdx.x / groups;
     const int c0 = (blockIdx.x % groups) * NRC;
@@ -246,13 +287,13 @@ __global__ void __launch_bounds__(NT)
     __syncthreads();
     if(!upper)
     {
-        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, 1, lda}, n, sb, nc);
-        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, lda, 1}, n, sb, nc);
+        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
     }
     else
     {
-        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc);
-        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc);
+        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
     }
     for(int e = threadIdx.x; e < n * nc; e += NT)
     {

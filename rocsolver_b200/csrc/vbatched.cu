@@ -125,10 +125,11 @@ __global__ void __launch_bounds__(NT)
         }
         if(v.mode != 1 && (v.mode == 2 || v.info[b] == 0))
         {
-            T* sb = reinterpret_cast<T*>(smem_raw);
+            T* sdiag = reinterpret_cast<T*>(smem_raw);
+            T* sb = sdiag + SDIAG_ELEMS;
             int* perm = reinterpret_cast<int*>(sb + (size_t)v.max_n * 4);
             getrs_dev<T, NT, 4>(0, n, v.nrhs[b], A[b], v.lda[b], v.ipiv[b], B[b], v.ldb[b], sb,
-                                perm);
+                                perm, sdiag);
         }
         __syncthreads();
     }
@@ -224,13 +225,13 @@ static int sm_count()
 template <typename T, int NT, int R, int JB, int TN>
 static rocblas_status run_vb(cudaStream_t s, VbArgs v, T* const* A, T* const* B)
 {
-    int cw = (int)((64 * 1024) / (sizeof(T) * JB));
-    cw = cw / TN * TN;
-    const int need = ((v.max_n + TN - 1) / TN) * TN;
-    if(need < cw)
-        cw = need < TN ? TN : need;
-    size_t smem = CtaLuSmem<T, NT, JB>::bytes(cw, R);
-    const size_t solve = sizeof(T) * (size_t)v.max_n * 4 + sizeof(int) * (size_t)v.max_n;
+    const int cwmax = sizeof(T) == 8 ? 64 : 128;
+    int cw = ((v.max_n + 31) / 32) * 32;
+    if(cw > cwmax)
+        cw = cwmax;
+    size_t smem = CtaLuSmem<T, NT, JB>::bytes(v.max_n, cw, R);
+    const size_t solve = sizeof(T) * ((size_t)v.max_n * 4 + SDIAG_ELEMS)
+                         + sizeof(int) * (size_t)v.max_n;
     if(solve > smem)
         smem = solve;
     auto k = vb_persistent_kernel<T, NT, R, JB, TN>;
