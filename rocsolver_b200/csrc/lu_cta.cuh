@@ -47,6 +47,7 @@ struct CtaLuSmem
         s += sizeof(T) * 32 * L11LD;            // L11
         s += sizeof(T) * 2 * NW * JB;           // candidate rows
         s += sizeof(T) * 2 * NW;                // candidate reciprocals
+        s += sizeof(T) * 2 * NW;                // candidate pivot values
         s += sizeof(K) * 2 * NW;                // candidate keys
         s += sizeof(int) * 2 * NW;              // candidate positions
         s += sizeof(int) * (size_t)R * NT;      // slot of each position
@@ -55,6 +56,58 @@ struct CtaLuSmem
         return (s + 15) & ~size_t(15);
     }
 };
+
+// Candidate rows are published shifted by one (dst[i] = v[i+1], dst[JB-1] = 0; the pivot
+// value itself goes to its own slot) with 16-byte vector stores, so that the rank-1
+// update, which pairs element i+1 of the pivot row with register i, reads aligned vectors.
+template <typename T, int JB>
+__device__ __forceinline__ void store_row_shifted(T* dst, const T (&v)[JB])
+{
+    auto at = [&](int i) { return i < JB ? v[i] : T(0); };
+    if constexpr(sizeof(T) == 8)
+    {
+#pragma unroll
+        for(int i = 0; i < JB; i += 2)
+            *reinterpret_cast<double2*>(dst + i) = make_double2(at(i + 1), at(i + 2));
+    }
+    else
+    {
+#pragma unroll
+        for(int i = 0; i < JB; i += 4)
+            *reinterpret_cast<float4*>(dst + i) =
+                make_float4(at(i + 1), at(i + 2), at(i + 3), at(i + 4));
+    }
+}
+// v[i] = fma(-l, row[i], v[i+1]) for i < JB-1 with row read as aligned vectors
+template <typename T, int JB>
+__device__ __forceinline__ void update_shift(T (&v)[JB], T l, const T* row)
+{
+    if constexpr(sizeof(T) == 8)
+    {
+#pragma unroll
+        for(int i = 0; i < JB; i += 2)
+        {
+            const double2 t = *reinterpret_cast<const double2*>(row + i);
+            if(i + 1 < JB)
+                v[i] = fma(-l, t.x, v[i + 1]);
+            if(i + 2 < JB)
+                v[i + 1] = fma(-l, t.y, v[i + 2]);
+        }
+    }
+    else
+    {
+#pragma unroll
+        for(int i = 0; i < JB; i += 4)
+        {
+            const float4 t = *reinterpret_cast<const float4*>(row + i);
+            const float e[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+            for(int u = 0; u < 4; ++u)
+                if(i + u + 1 < JB)
+                    v[i + u] = fmaf(-l, e[u], v[i + u + 1]);
+        }
+    }
+}
 
 // ---------------------------------------------------------------------------------------
 // Warp tile products.  acc (32 x 32 tile) += A * B over k < K where A(r, k) = sA[k*lda_s +
@@ -187,7 +240,8 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
     T* sL11 = sLi + 32 * SM::LDI;                      // [32][L11LD]
     T* cand = sL11 + 32 * SM::L11LD;                   // [2][NW][JB]
     T* crcp = cand + 2 * NW * JB;                      // [2][NW]
-    K* ckey = reinterpret_cast<K*>(crcp + 2 * NW);     // [2][NW]
+    T* cpiv = crcp + 2 * NW;                           // [2][NW]
+    K* ckey = reinterpret_cast<K*>(cpiv + 2 * NW);     // [2][NW]
     int* crow = reinterpret_cast<int*>(ckey + 2 * NW); // [2][NW]
     int* slotof = crow + 2 * NW;                       // [R*NT]
     int* moved = slotof + R * NT;                      // [2*JB]
@@ -215,7 +269,16 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             for(int c = 0; c < JB; ++c)
                 pv[q][c] = (r < mp && c < jb) ? a[ix(j0 + r, j0 + c, lda)] : T(0);
         }
-        // ---------------- factor the panel: rolled column loop, one barrier per column
+        // ---------------- factor the panel: rolled column loop, one barrier per column.
+        // Warps whose slots all lie below the panel's last row only keep the barrier.
+        const int nact = min(NW, (mp + 31) / 32);
+        if(warp >= nact)
+        {
+#pragma unroll 1
+            for(int c = 0; c < jb; ++c)
+                __syncthreads();
+        }
+        else
 #pragma unroll 1
         for(int c = 0; c < jb; ++c)
         {
@@ -249,10 +312,9 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                     for(int q = 0; q < R; ++q)
                         if(lrow[q] == wr && tid + q * NT < mp)
                         {
-#pragma unroll
-                            for(int i = 0; i < JB; ++i)
-                                cb[warp * JB + i] = pv[q][i];
+                            store_row_shifted<T, JB>(cb + warp * JB, pv[q]);
                             const T p = pv[q][0];
+                            cpiv[buf * NW + warp] = p;
                             crcp[buf * NW + warp] = p != T(0) ? T(1) / p : T(0);
                         }
                 }
@@ -268,6 +330,8 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
 #pragma unroll
                 for(int w = 0; w < NW; ++w)
                 {
+                    if(w >= nact)
+                        break;
                     const int rr = crow[buf * NW + w];
                     const K kw = ckey[buf * NW + w];
                     if(rr != INT_MAX && (gw < 0 || kw > gk || (kw == gk && rr < gr)))
@@ -285,16 +349,15 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                 for(int q = 0; q < R; ++q)
                     if(lrow[q] == c && tid + q * NT < mp)
                     {
-#pragma unroll
-                        for(int i = 0; i < JB; ++i)
-                            cb[i] = pv[q][i];
+                        store_row_shifted<T, JB>(cb, pv[q]);
                         const T p = pv[q][0];
+                        cpiv[buf * NW] = p;
                         crcp[buf * NW] = p != T(0) ? T(1) / p : T(0);
                     }
                 __syncthreads();
             }
-            const T* prowv = cb + gw * JB;
-            const T pivv = prowv[0];
+            const T* prowv = cb + gw * JB; // pivot row, shifted by one
+            const T pivv = cpiv[buf * NW + gw];
             const T rcp = crcp[buf * NW + gw];
             if(tid == 0)
                 spiv[c] = prow;
@@ -328,9 +391,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                         const T x = pv[q][0];
                         const T l = mode == 1 ? x * rcp : (mode == 2 ? x / pivv : x);
                         sP[c * ldp + slot] = -l;
-#pragma unroll
-                        for(int i = 0; i + 1 < JB; ++i)
-                            pv[q][i] = fma(-l, prowv[i + 1], pv[q][i + 1]);
+                        update_shift<T, JB>(pv[q], l, prowv);
                     }
                 }
             }
