@@ -799,6 +799,32 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_vbatched(rocblas_handle handle,
     const rocblas_int max_nrhs,
     const rocblas_int batch_count);
 
+/* Variable-size gesv that never allocates device memory (no counterpart in the
+ * reference).  Same arguments and per-member results as rocsolver_dgesv_vbatched.  That
+ * routine takes a little scratch (its work list) from the handle's workspace, which the
+ * library allocates with cudaMalloc on first use; callers that may not allocate (code
+ * running while a memory pool owns the device memory, allocation-free real-time loops,
+ * plugins whose host framework forbids device allocations) use this variant, which keeps
+ * the scratch in a fixed ~4 MiB array in the library's device memory (held on every GPU
+ * that loads the library until the process exits).
+ *   - batch_count is limited to 1048576 members; larger batches return invalid_size.
+ *   - All calls share the array: calls that overlap on the GPU race; order them on one
+ *     stream.  Nothing carries over between calls (the work list is rebuilt each call).
+ *   - The first call on a device looks up the array's device address; make that first
+ *     call before any stream capture on that device. */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_vbatched_noalloc(rocblas_handle handle,
+    const rocblas_int* n,
+    const rocblas_int* nrhs,
+    double* const A[],
+    const rocblas_int* lda,
+    rocblas_int* const ipiv[],
+    double* const B[],
+    const rocblas_int* ldb,
+    rocblas_int* info,
+    const rocblas_int max_n,
+    const rocblas_int max_nrhs,
+    const rocblas_int batch_count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,7 @@ for _p in "sd":
     _EXTRA[f"rocsolver_{_p}getrf_vbatched"] = (_c.c_int, [H, P, P, P, P, P, I, I])
     _EXTRA[f"rocsolver_{_p}getrs_vbatched"] = (_c.c_int, [H, P, P, P, P, P, P, P, I, I, I])
     _EXTRA[f"rocsolver_{_p}gesv_vbatched"] = (_c.c_int, [H, P, P, P, P, P, P, P, P, I, I, I])
+_EXTRA["rocsolver_dgesv_vbatched_noalloc"] = (_c.c_int, [H, P, P, P, P, P, P, P, P, I, I, I])
 
 _HANDLE_FUNCS = {
     "rocblas_create_handle": (_c.c_int, [_c.POINTER(H)]),
