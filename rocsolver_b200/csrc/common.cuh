@@ -68,11 +68,14 @@ template <>
 struct Lim<double>
 {
     static __device__ __forceinline__ double sfmin() { return DBL_MIN; }
+    // correctly rounded reciprocal (same value as 1.0 / x)
+    static __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
 };
 template <>
 struct Lim<float>
 {
     static __device__ __forceinline__ float sfmin() { return FLT_MIN; }
+    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 };
 
 // ---------------------------------------------------------------------------------------

@@ -76,7 +76,7 @@ static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, in
 {
     // trailing column chunk: multiple of 32 columns (FP64: 64, FP32: 128 at most), so that
     // two CTAs fit in an SM's shared memory
-    const int cwmax = sizeof(T) == 8 ? 64 : 128;
+    const int cwmax = sizeof(T) == 8 ? LU_CW_F64 : LU_CW_F32;
     int cw = ((n + 31) / 32) * 32;
     if(cw > cwmax)
         cw = cwmax;
@@ -106,6 +106,10 @@ static rocblas_status getrf_dispatch(cudaStream_t s, int m, int n, Batch<T> A, i
         return run_getrf_cta<T, 64, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
     if(m <= 128)
         return run_getrf_cta<T, 128, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+    // FP32: 128-thread CTAs with two rows per thread (three CTAs per SM); FP64 keeps
+    // 256 threads (its two-row panel would not fit the register budget)
+    if(sizeof(T) == 4 && m > 128 && m <= 256)
+        return run_getrf_cta<T, 128, 2, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
     if(m <= 256)
         return run_getrf_cta<T, 256, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
     if(m <= 512)

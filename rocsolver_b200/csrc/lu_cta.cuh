@@ -29,6 +29,16 @@
 
 namespace rsb {
 
+#ifndef LU_MIN_BLOCKS
+#define LU_MIN_BLOCKS 2
+#endif
+#ifndef LU_CW_F64
+#define LU_CW_F64 64
+#endif
+#ifndef LU_CW_F32
+#define LU_CW_F32 128
+#endif
+
 template <typename T, int NT, int JB>
 struct CtaLuSmem
 {
@@ -315,7 +325,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                             store_row_shifted<T, JB>(cb + warp * JB, pv[q]);
                             const T p = pv[q][0];
                             cpiv[buf * NW + warp] = p;
-                            crcp[buf * NW + warp] = p != T(0) ? T(1) / p : T(0);
+                            crcp[buf * NW + warp] = p != T(0) ? Lim<T>::rcp(p) : T(0);
                         }
                 }
                 if(lane == 0)
@@ -324,20 +334,29 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                     crow[buf * NW + warp] = wr;
                 }
                 __syncthreads();
-                K gk = 0;
-                int gr = INT_MAX;
-                gw = -1;
+                // every warp's record is read up front, then reduced: largest key,
+                // smallest position on ties (LAPACK: first index of the maximum)
+                K kw[NW];
+                int rw[NW];
 #pragma unroll
                 for(int w = 0; w < NW; ++w)
                 {
-                    if(w >= nact)
-                        break;
-                    const int rr = crow[buf * NW + w];
-                    const K kw = ckey[buf * NW + w];
-                    if(rr != INT_MAX && (gw < 0 || kw > gk || (kw == gk && rr < gr)))
+                    kw[w] = ckey[buf * NW + w];
+                    rw[w] = w < nact ? crow[buf * NW + w] : INT_MAX;
+                }
+                K gk = kw[0];
+                int gr = rw[0];
+                gw = 0;
+#pragma unroll
+                for(int w = 1; w < NW; ++w)
+                {
+                    const bool better = rw[w] != INT_MAX
+                                        && (gr == INT_MAX || kw[w] > gk
+                                            || (kw[w] == gk && rw[w] < gr));
+                    if(better)
                     {
-                        gk = kw;
-                        gr = rr;
+                        gk = kw[w];
+                        gr = rw[w];
                         gw = w;
                     }
                 }
@@ -352,7 +371,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                         store_row_shifted<T, JB>(cb, pv[q]);
                         const T p = pv[q][0];
                         cpiv[buf * NW] = p;
-                        crcp[buf * NW] = p != T(0) ? T(1) / p : T(0);
+                        crcp[buf * NW] = p != T(0) ? Lim<T>::rcp(p) : T(0);
                     }
                 __syncthreads();
             }
@@ -560,7 +579,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
 }
 
 template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, LU_MIN_BLOCKS)
     getrf_cta_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
                      int cw, Gate gate)
 {

@@ -26,6 +26,9 @@
 namespace rsb {
 
 constexpr int DSGESV_ITERMAX = 10;
+// refinement solves use inverted diagonal blocks up to this order (their shared memory
+// grows as n); larger orders use the staged-block substitution
+constexpr int REFINE_BLOCKINV_MAXN = 512;
 
 __global__ void __launch_bounds__(256)
     dsgesv_convert_kernel(int n, Batch<double> A, int lda, float* a32, double* anrm, int* flag,
@@ -89,6 +92,145 @@ __device__ __forceinline__ double block_max(double v, double* red)
     return m;
 }
 
+// ---- triangular solves with the FP32 factors through inverted 32x32 diagonal blocks
+constexpr int BI_LD = 33;
+constexpr int BI_ELEMS = 32 * BI_LD;
+
+// Invert the diagonal blocks of the FP32 LU once per matrix: blocks 0..nblk-1 of L (unit
+// lower) and nblk..2*nblk-1 of U (upper).  One warp per block: the block is staged
+// row-major in its slot, lane j computes column j of the inverse by substitution in
+// registers, then the lanes overwrite the block with the inverse.  Partial blocks are
+// padded with the identity.
+template <int NT>
+__device__ void invert_diag_blocks(const float* lu, int n, float* sinv)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nblk = (n + 31) / 32;
+    for(int t = warp; t < 2 * nblk; t += NT / 32)
+    {
+        const bool upper = t >= nblk;
+        const int kb = (upper ? t - nblk : t) * 32, nb = min(32, n - kb);
+        float* blk = sinv + t * BI_ELEMS;
+#pragma unroll 4
+        for(int k = 0; k < 32; ++k)
+        {
+            const int i = lane;
+            float v;
+            if(i >= nb || k >= nb)
+                v = i == k ? 1.f : 0.f;
+            else if(!upper)
+                v = i > k ? lu[(kb + i) + (size_t)(kb + k) * n] : (i == k ? 1.f : 0.f);
+            else
+                v = i <= k ? lu[(kb + i) + (size_t)(kb + k) * n] : 0.f;
+            blk[i * BI_LD + k] = v;
+        }
+        __syncwarp();
+        float x[32];
+#pragma unroll
+        for(int i = 0; i < 32; ++i)
+            x[i] = i == lane ? 1.f : 0.f;
+        if(!upper)
+        {
+#pragma unroll
+            for(int k = 0; k < 32; ++k)
+#pragma unroll
+                for(int i = k + 1; i < 32; ++i)
+                    x[i] = fmaf(-blk[i * BI_LD + k], x[k], x[i]);
+        }
+        else
+        {
+#pragma unroll
+            for(int k = 31; k >= 0; --k)
+            {
+                x[k] = x[k] / blk[k * BI_LD + k];
+#pragma unroll
+                for(int i = 0; i < k; ++i)
+                    x[i] = fmaf(-blk[i * BI_LD + k], x[k], x[i]);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for(int i = 0; i < 32; ++i)
+            blk[i * BI_LD + lane] = x[i];
+        __syncwarp();
+    }
+}
+
+// Solve (forward: L, unit lower; else U) for nc columns of s (ld n) using the inverted
+// diagonal blocks: per 32-block, warp 0 applies the block inverse (a 32x32 mat-vec, no
+// serial chain), then all threads apply the block to the remaining rows.
+template <int NT, int NRC>
+__device__ void blockinv_sweep(bool forward, const float* lu, int n, const float* sinv,
+                               float* s, int nc)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nblk = (n + 31) / 32;
+    for(int bi = 0; bi < nblk; ++bi)
+    {
+        const int blkid = forward ? bi : nblk - 1 - bi;
+        const int kb = blkid * 32, nb = min(32, n - kb);
+        const float* inv = sinv + (forward ? blkid : nblk + blkid) * BI_ELEMS;
+        if(warp == 0)
+        {
+            float y[NRC];
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                y[c] = 0.f;
+#pragma unroll 8
+            for(int j = 0; j < 32; ++j)
+            {
+                const float mij = inv[lane * BI_LD + j];
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                    if(c < nc && j < nb)
+                        y[c] = fmaf(mij, s[kb + j + c * n], y[c]);
+            }
+            __syncwarp();
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                if(c < nc && lane < nb)
+                    s[kb + lane + c * n] = y[c];
+        }
+        __syncthreads();
+        const int r0 = forward ? kb + nb : 0;
+        const int r1 = forward ? n : kb;
+        for(int i = r0 + tid; i < r1; i += NT)
+        {
+            float acc[NRC];
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                acc[c] = c < nc ? s[i + c * n] : 0.f;
+            if(nb == 32)
+            {
+                float mv[32];
+#pragma unroll
+                for(int k = 0; k < 32; ++k)
+                    mv[k] = lu[i + (size_t)(kb + k) * n];
+#pragma unroll
+                for(int k = 0; k < 32; ++k)
+#pragma unroll
+                    for(int c = 0; c < NRC; ++c)
+                        acc[c] = fmaf(-mv[k], s[kb + k + c * n], acc[c]);
+            }
+            else
+            {
+                for(int k = 0; k < nb; ++k)
+                {
+                    const float mik = lu[i + (size_t)(kb + k) * n];
+#pragma unroll
+                    for(int c = 0; c < NRC; ++c)
+                        acc[c] = fmaf(-mik, s[kb + k + c * n], acc[c]);
+                }
+            }
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                if(c < nc)
+                    s[i + c * n] = acc[c];
+        }
+        __syncthreads();
+    }
+}
+
 template <int NT, int NRC>
 __global__ void __launch_bounds__(NT)
     dsgesv_refine_kernel(int n, int nrhs, Batch<double> A, int lda, const float* lu32,
@@ -103,6 +245,8 @@ __global__ void __launch_bounds__(NT)
     float* sdiag = reinterpret_cast<float*>(red + NT / 32); // staged diagonal blocks
     float* s32 = sdiag + SDIAG_ELEMS;                       // n x NRC
     int* perm = reinterpret_cast<int*>(s32 + (size_t)n * NRC);
+    float* sinv = reinterpret_cast<float*>(perm + ((n + 3) & ~3)); // [2*nblk][32x33]
+    const bool blockinv = n <= REFINE_BLOCKINV_MAXN;
     __shared__ int bad;
 
     const int64_t b = blockIdx.x;
@@ -122,6 +266,11 @@ __global__ void __launch_bounds__(NT)
     double* x = X.at(b);
     const float* lu = lu32 + (size_t)b * n * n;
     build_perm(ipiv + b * strideP, n, perm);
+    if(blockinv)
+    {
+        invert_diag_blocks<NT>(lu, n, sinv);
+        __syncthreads();
+    }
     const double cte = anrm[b] * (DBL_EPSILON * 0.5) * sqrt((double)n);
     const int tot = n * nrhs;
     for(int e = tid; e < tot; e += NT)
@@ -148,8 +297,18 @@ __global__ void __launch_bounds__(NT)
                 s32[i + c * n] = (float)v;
             }
             __syncthreads();
-            block_sweep<float, NT, NRC>(true, true, TriView<float>{lu, 1, n}, n, s32, nc, sdiag);
-            block_sweep<float, NT, NRC>(false, false, TriView<float>{lu, 1, n}, n, s32, nc, sdiag);
+            if(blockinv)
+            {
+                blockinv_sweep<NT, NRC>(true, lu, n, sinv, s32, nc);
+                blockinv_sweep<NT, NRC>(false, lu, n, sinv, s32, nc);
+            }
+            else
+            {
+                block_sweep<float, NT, NRC>(true, true, TriView<float>{lu, 1, n}, n, s32, nc,
+                                            sdiag);
+                block_sweep<float, NT, NRC>(false, false, TriView<float>{lu, 1, n}, n, s32, nc,
+                                            sdiag);
+            }
             for(int e = tid; e < n * nc; e += NT)
             {
                 const int i = e % n, c = e / n;
@@ -257,8 +416,11 @@ __global__ void mark_all_kernel(int bc, int* flag, int* info, int* iter)
 
 static size_t refine_smem(int n, int nrhs, int NRC, int NT)
 {
+    const size_t nblk = (n + 31) / 32;
+    const size_t inv = n <= REFINE_BLOCKINV_MAXN ? 2 * nblk * BI_ELEMS : 0;
     return sizeof(double) * (2 * (size_t)n * nrhs + NT / 32)
-           + sizeof(float) * ((size_t)n * NRC + SDIAG_ELEMS) + sizeof(int) * (size_t)n;
+           + sizeof(float) * ((size_t)n * NRC + SDIAG_ELEMS + inv)
+           + sizeof(int) * (size_t)((n + 3) & ~3);
 }
 
 size_t dsgesv_workspace(int n, int nrhs, int bc)

@@ -225,7 +225,7 @@ static int sm_count()
 template <typename T, int NT, int R, int JB, int TN>
 static rocblas_status run_vb(cudaStream_t s, VbArgs v, T* const* A, T* const* B)
 {
-    const int cwmax = sizeof(T) == 8 ? 64 : 128;
+    const int cwmax = sizeof(T) == 8 ? LU_CW_F64 : LU_CW_F32;
     int cw = ((v.max_n + 31) / 32) * 32;
     if(cw > cwmax)
         cw = cwmax;
