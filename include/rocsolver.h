@@ -825,6 +825,21 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_vbatched_noalloc(rocblas_handle 
     const rocblas_int max_nrhs,
     const rocblas_int batch_count);
 
+/* ---- Kernel configuration table (no counterpart in the reference, whose block sizes and
+ * kernel switch points are compile-time constants: library/src/include/ideal_sizes.hpp:
+ * 166-240, docs/design/tuning.rst:20-31).  The table is text, one entry per line:
+ *   getrf    <s|d> <m_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold>
+ *   vbatched <s|d> <n_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold> <ctas_per_sm>
+ * It is written by the autotuner (python -m rocsolver_b200.tune) and read when the first
+ * handle is created, from $ROCSOLVER_B200_TUNING or else tuning_b200.txt beside the
+ * library.  Entries that name an unavailable configuration fall back to the built-in
+ * choice; results do not depend on the table, only speed does. */
+ROCSOLVER_EXPORT rocblas_status rocsolver_b200_tuning_set(const char* text);   /* replace */
+ROCSOLVER_EXPORT rocblas_status rocsolver_b200_tuning_load(const char* path);  /* from file */
+/* Writes the active table (NUL-terminated, truncated to len) and returns its full size
+ * including the NUL. */
+ROCSOLVER_EXPORT size_t rocsolver_b200_tuning_get(char* buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,9 @@ for _p in "sd":
     _EXTRA[f"rocsolver_{_p}getrs_vbatched"] = (_c.c_int, [H, P, P, P, P, P, P, P, I, I, I])
     _EXTRA[f"rocsolver_{_p}gesv_vbatched"] = (_c.c_int, [H, P, P, P, P, P, P, P, P, I, I, I])
 _EXTRA["rocsolver_dgesv_vbatched_noalloc"] = (_c.c_int, [H, P, P, P, P, P, P, P, P, I, I, I])
+_EXTRA["rocsolver_b200_tuning_set"] = (_c.c_int, [_c.c_char_p])
+_EXTRA["rocsolver_b200_tuning_load"] = (_c.c_int, [_c.c_char_p])
+_EXTRA["rocsolver_b200_tuning_get"] = (_c.c_size_t, [_c.c_char_p, _c.c_size_t])
 
 _HANDLE_FUNCS = {
     "rocblas_create_handle": (_c.c_int, [_c.POINTER(H)]),
@@ -171,3 +174,17 @@ def call(name, *args):
 def check(status, what=""):
     if status != SUCCESS:
         raise RuntimeError(f"{what}: rocblas_status_{STATUS_NAMES[status]}")
+
+
+def tuning_table():
+    """The active kernel configuration table as text (tuning.h format)."""
+    l = lib()
+    size = l.rocsolver_b200_tuning_get(None, 0)
+    buf = _c.create_string_buffer(size)
+    l.rocsolver_b200_tuning_get(buf, size)
+    return buf.value.decode()
+
+
+def set_tuning_table(text):
+    """Replace the active kernel configuration table; returns the rocblas status."""
+    return lib().rocsolver_b200_tuning_set(text.encode())

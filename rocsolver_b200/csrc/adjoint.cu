@@ -15,7 +15,7 @@
 namespace rsb {
 
 template <typename T, int NT, int NRC>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 1)
     solve_adjoint_kernel(int kind, int n, int nrhs, Batch<T> A, int lda, const int* ipiv,
                          int64_t strideP, Batch<T> X, int ldx, Batch<T> G, int ldg, Batch<T> GA,
                          int ldga, Batch<T> GB, int ldgb)

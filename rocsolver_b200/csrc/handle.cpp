@@ -7,6 +7,7 @@
 #include <new>
 
 #include "handle.h"
+#include "tuning.h"
 
 namespace rsb {
 
@@ -90,6 +91,7 @@ rocblas_status rocblas_create_handle(rocblas_handle* handle)
 {
     if(!handle)
         return rocblas_status_invalid_pointer;
+    rsb::tuning_load_default_once();
     _rocblas_handle* h = new(std::nothrow) _rocblas_handle();
     if(!h)
         return rocblas_status_memory_error;

@@ -2,12 +2,14 @@
 //
 // Kernel selection by size replaces the reference's compile-time tuning tables
 // (library/src/include/ideal_sizes.hpp:208-240 getrf, :166-180 potrf;
-// roclapack_getf2.hpp:181-276 select_spkernel).
+// roclapack_getf2.hpp:181-276 select_spkernel): the CTA LU configuration comes from the
+// run-time tuning table (tuning.h) when it has an entry, else from the built-in choice.
 #include "chol.cuh"
 #include "launch.h"
 #include "lu_cta.cuh"
 #include "lu_small.cuh"
 #include "trsv.cuh"
+#include "tuning.h"
 
 namespace rsb {
 
@@ -70,22 +72,60 @@ static void run_getrf_warp(cudaStream_t s, int m, int n, Batch<T> A, int lda, in
                                                                        info, bc, g);
 }
 
-template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
+// cw: trailing column chunk (multiple of 32); 0 picks the default (FP64: 64, FP32: 128 at
+// most, so that two CTAs fit in an SM's shared memory).  *ran = false when the variant
+// cannot take this size (more rows than threads x rows per thread, or too much shared
+// memory): the caller then uses the built-in choice.
+template <typename T, int NT, int R, int JB, bool PIVOT>
 static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, int lda,
-                                    int* ipiv, int64_t sP, int* info, int bc, Gate g)
+                                    int* ipiv, int64_t sP, int* info, int bc, Gate g, int cw,
+                                    int fold, bool* ran = nullptr)
 {
-    // trailing column chunk: multiple of 32 columns (FP64: 64, FP32: 128 at most), so that
-    // two CTAs fit in an SM's shared memory
+    if(ran)
+        *ran = false;
+    if(m > NT * R)
+        return rocblas_status_not_implemented;
     const int cwmax = sizeof(T) == 8 ? LU_CW_F64 : LU_CW_F32;
-    int cw = ((n + 31) / 32) * 32;
-    if(cw > cwmax)
+    const int nround = ((n + 31) / 32) * 32;
+    if(cw <= 0)
         cw = cwmax;
+    cw = ((cw + 31) / 32) * 32;
+    if(cw > nround)
+        cw = nround;
     const size_t smem = CtaLuSmem<T, NT, JB>::bytes(m, cw, R);
-    auto k = getrf_cta_kernel<T, NT, R, JB, TN, PIVOT>;
+    if(smem > 227 * 1024)
+        return rocblas_status_not_implemented;
+    auto k = getrf_cta_kernel<T, NT, R, JB, 8, PIVOT>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
-    k<<<bc, NT, smem, s>>>(m, n, A, lda, ipiv, sP, info, cw, g);
+    if(ran)
+        *ran = true;
+    k<<<bc, NT, smem, s>>>(m, n, A, lda, ipiv, sP, info, cw, fold, g);
     return launch_status();
+}
+
+// the compiled CTA variants a tuning entry may name: (threads, rows per thread, panel width)
+template <typename T, bool PIVOT>
+static rocblas_status run_getrf_tuned(const LuCfg& c, cudaStream_t s, int m, int n,
+                                      Batch<T> A, int lda, int* ipiv, int64_t sP, int* info,
+                                      int bc, Gate g, bool* ran)
+{
+    *ran = false;
+#define RSB_LU_VARIANT(NT_, R_, JB_)                                                          \
+    if(c.nt == NT_ && c.r == R_ && c.jb == JB_)                                                \
+        return run_getrf_cta<T, NT_, R_, JB_, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g,  \
+                                                     c.cw, c.fold, ran);
+    RSB_LU_VARIANT(64, 1, 32)
+    RSB_LU_VARIANT(128, 1, 32)
+    RSB_LU_VARIANT(128, 2, 32)
+    RSB_LU_VARIANT(128, 2, 16)
+    RSB_LU_VARIANT(128, 4, 16)
+    RSB_LU_VARIANT(256, 1, 32)
+    RSB_LU_VARIANT(256, 2, 16)
+    RSB_LU_VARIANT(256, 4, 8)
+    RSB_LU_VARIANT(256, 8, 4)
+#undef RSB_LU_VARIANT
+    return rocblas_status_not_implemented;
 }
 
 template <typename T, bool PIVOT>
@@ -102,22 +142,32 @@ static rocblas_status getrf_dispatch(cudaStream_t s, int m, int n, Batch<T> A, i
             run_getrf_warp<T, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
         return launch_status();
     }
+    LuCfg c;
+    if(tuned_getrf(sizeof(T) == 8 ? 'd' : 's', m, &c))
+    {
+        bool ran = false;
+        const rocblas_status st =
+            run_getrf_tuned<T, PIVOT>(c, s, m, n, A, lda, ipiv, sP, info, bc, g, &ran);
+        if(ran)
+            return st;
+    }
+    // built-in choice (used when no tuning table is installed)
     if(m <= 64)
-        return run_getrf_cta<T, 64, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+        return run_getrf_cta<T, 64, 1, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
     if(m <= 128)
-        return run_getrf_cta<T, 128, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+        return run_getrf_cta<T, 128, 1, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
     // FP32: 128-thread CTAs with two rows per thread (three CTAs per SM); FP64 keeps
     // 256 threads (its two-row panel would not fit the register budget)
-    if(sizeof(T) == 4 && m > 128 && m <= 256)
-        return run_getrf_cta<T, 128, 2, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+    if(sizeof(T) == 4 && m <= 256)
+        return run_getrf_cta<T, 128, 2, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
     if(m <= 256)
-        return run_getrf_cta<T, 256, 1, 32, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+        return run_getrf_cta<T, 256, 1, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
     if(m <= 512)
-        return run_getrf_cta<T, 256, 2, 16, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+        return run_getrf_cta<T, 256, 2, 16, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
     if(m <= 1024)
-        return run_getrf_cta<T, 256, 4, 8, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+        return run_getrf_cta<T, 256, 4, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
     if(m <= MAX_CTA_ROWS)
-        return run_getrf_cta<T, 256, 8, 4, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+        return run_getrf_cta<T, 256, 8, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
     return rocblas_status_not_implemented;
 }
 
@@ -152,19 +202,35 @@ static void getrs_warp_nrc(cudaStream_t s, int trans, int n, int nrhs, Batch<T> 
         run_getrs_warp<T, NMAX, 4>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, g);
 }
 
+template <typename T, int NT, int NRC>
+static rocblas_status run_getrs_cta_nt(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A,
+                                       int lda, const int* ipiv, int64_t sP, Batch<T> B,
+                                       int ldb, const int* skip, int bc, Gate g)
+{
+    const size_t smem = sizeof(T) * ((size_t)n * NRC + SDIAG_ELEMS) + sizeof(int) * (size_t)n;
+    auto k = getrs_cta_kernel<T, NT, NRC>;
+    if(!set_smem(k, smem))
+        return rocblas_status_internal_error;
+    const int64_t groups = (nrhs + NRC - 1) / NRC;
+    k<<<(unsigned)(bc * groups), NT, smem, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip,
+                                                g);
+    return launch_status();
+}
+
+// CTA size follows n: one thread per row for the off-diagonal updates
 template <typename T, int NRC>
 static rocblas_status run_getrs_cta(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A,
                                     int lda, const int* ipiv, int64_t sP, Batch<T> B, int ldb,
                                     const int* skip, int bc, Gate g)
 {
-    const size_t smem = sizeof(T) * ((size_t)n * NRC + SDIAG_ELEMS) + sizeof(int) * (size_t)n;
-    auto k = getrs_cta_kernel<T, 256, NRC>;
-    if(!set_smem(k, smem))
-        return rocblas_status_internal_error;
-    const int64_t groups = (nrhs + NRC - 1) / NRC;
-    k<<<(unsigned)(bc * groups), 256, smem, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip,
-                                                 g);
-    return launch_status();
+    if(n <= 64)
+        return run_getrs_cta_nt<T, 64, NRC>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip,
+                                            bc, g);
+    if(n <= 128)
+        return run_getrs_cta_nt<T, 128, NRC>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip,
+                                             bc, g);
+    return run_getrs_cta_nt<T, 256, NRC>(s, trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc,
+                                         g);
 }
 
 template <typename T>
@@ -255,17 +321,28 @@ rocblas_status launch_potrf(cudaStream_t s, int upper, int n, Batch<T> A, int ld
     return rocblas_status_not_implemented;
 }
 
+template <typename T, int NT, int NRC>
+static rocblas_status run_potrs_nt(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A,
+                                   int lda, Batch<T> B, int ldb, const int* skip, int bc)
+{
+    const size_t smem = sizeof(T) * ((size_t)n * NRC + SDIAG_ELEMS);
+    auto k = potrs_cta_kernel<T, NT, NRC>;
+    if(!set_smem(k, smem))
+        return rocblas_status_internal_error;
+    const int64_t groups = (nrhs + NRC - 1) / NRC;
+    k<<<(unsigned)(bc * groups), NT, smem, s>>>(upper, n, nrhs, A, lda, B, ldb, skip);
+    return launch_status();
+}
+
 template <typename T, int NRC>
 static rocblas_status run_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A,
                                 int lda, Batch<T> B, int ldb, const int* skip, int bc)
 {
-    const size_t smem = sizeof(T) * ((size_t)n * NRC + SDIAG_ELEMS);
-    auto k = potrs_cta_kernel<T, 256, NRC>;
-    if(!set_smem(k, smem))
-        return rocblas_status_internal_error;
-    const int64_t groups = (nrhs + NRC - 1) / NRC;
-    k<<<(unsigned)(bc * groups), 256, smem, s>>>(upper, n, nrhs, A, lda, B, ldb, skip);
-    return launch_status();
+    if(n <= 64)
+        return run_potrs_nt<T, 64, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
+    if(n <= 128)
+        return run_potrs_nt<T, 128, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
+    return run_potrs_nt<T, 256, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
 }
 
 template <typename T>

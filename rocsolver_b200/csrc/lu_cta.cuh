@@ -16,12 +16,14 @@
 //     and U rows are parked in shared memory by slot, which is also the A operand of
 //     the trailing update.
 //   * The panel's interchanges reach the other columns as a warp-local gather/scatter of
-//     the moved rows (at most 2*JB) per column: no CTA barrier inside.
+//     the moved rows (at most 2*JB) per column, or (fold) only the columns left of it, the
+//     trailing update reading each right-hand position from its source row.
 //   * U12 = L11^{-1} A12 as a small GEMM: one warp inverts the unit-lower L11 once per
 //     panel, then warps multiply 32-column tiles in place in shared memory.
 //   * A22 -= L21 U12 as 32x32 warp tiles; A22 is streamed from L2/HBM once per panel.
 //   FP64 tiles run on the FP64 tensor path (mma.sync.m8n8k4.f64, 256 FMAs per instruction;
-//   tcgen05 has no FP64 kind); FP32 tiles are 4x8 register tiles per lane.  Shared-memory
+//   tcgen05 has no FP64 kind); FP32 tiles are 4x8 register tiles per lane updated with
+//   packed fma.rn.f32x2 (two FMAs per instruction).  Shared-memory
 //   operands have leading dimension = 4 (mod 16) elements (bank-conflict-free fragments).
 #pragma once
 
@@ -182,17 +184,31 @@ struct WarpTile<double>
     }
 };
 
+// acc(i, 2p..2p+1) += l(i) * (u(2p), u(2p+1)) as one packed FP32 FMA (fma.rn.f32x2: each
+// half rounds exactly like fmaf, so results equal the scalar form bit for bit)
+__device__ __forceinline__ void fma2(float2& acc, float l, float u0, float u1)
+{
+    asm("{\n\t.reg .b64 pa, pb, pc;\n\t"
+        "mov.b64 pa, {%2, %2};\n\t"
+        "mov.b64 pb, {%3, %4};\n\t"
+        "mov.b64 pc, {%0, %1};\n\t"
+        "fma.rn.f32x2 pc, pa, pb, pc;\n\t"
+        "mov.b64 {%0, %1}, pc;\n\t}"
+        : "+f"(acc.x), "+f"(acc.y)
+        : "f"(l), "f"(u0), "f"(u1));
+}
+
 template <>
 struct WarpTile<float>
 {
-    float acc[4][8];
+    float2 acc[4][4]; // rows rg*4+i, columns cg*8 + 2p + {0,1}
     __device__ __forceinline__ void zero()
     {
 #pragma unroll
         for(int i = 0; i < 4; ++i)
 #pragma unroll
-            for(int j = 0; j < 8; ++j)
-                acc[i][j] = 0.f;
+            for(int p = 0; p < 4; ++p)
+                acc[i][p] = make_float2(0.f, 0.f);
     }
     template <int K>
     __device__ __forceinline__ void mma(const float* sA, int lda_s, const int (&arow)[4],
@@ -208,12 +224,14 @@ struct WarpTile<float>
                 lv[i] = sA[k * lda_s + arow[i]];
             const float4 u0 = *reinterpret_cast<const float4*>(sB + k * ldb_s + c0 + cg * 8);
             const float4 u1 = *reinterpret_cast<const float4*>(sB + k * ldb_s + c0 + cg * 8 + 4);
-            const float uv[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
 #pragma unroll
             for(int i = 0; i < 4; ++i)
-#pragma unroll
-                for(int j = 0; j < 8; ++j)
-                    acc[i][j] = fmaf(lv[i], uv[j], acc[i][j]);
+            {
+                fma2(acc[i][0], lv[i], u0.x, u0.y);
+                fma2(acc[i][1], lv[i], u0.z, u0.w);
+                fma2(acc[i][2], lv[i], u1.x, u1.y);
+                fma2(acc[i][3], lv[i], u1.z, u1.w);
+            }
         }
     }
     template <typename F>
@@ -223,8 +241,11 @@ struct WarpTile<float>
 #pragma unroll
         for(int i = 0; i < 4; ++i)
 #pragma unroll
-            for(int j = 0; j < 8; ++j)
-                f(rg * 4 + i, cg * 8 + j, acc[i][j]);
+            for(int p = 0; p < 4; ++p)
+            {
+                f(rg * 4 + i, cg * 8 + 2 * p, acc[i][p].x);
+                f(rg * 4 + i, cg * 8 + 2 * p + 1, acc[i][p].y);
+            }
     }
     static __device__ __forceinline__ int frag_row(int i)
     {
@@ -234,12 +255,16 @@ struct WarpTile<float>
 
 // Factor one m x n matrix with the whole CTA.  smem_raw must hold CtaLuSmem::bytes(m, cw, R);
 // m <= R*NT; cw is a multiple of 32.  Writes ipiv (1-based, PIVOT only) and *info_out.
+// fold: apply each panel's row interchanges to the columns right of it inside the trailing
+// update instead of swapping them in memory first (a tuning choice; same results).
 // Called by all threads of the CTA.
 template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
 __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* piv_out,
-                                              int* info_out, int cw, unsigned char* smem_raw)
+                                              int* info_out, int cw, bool fold,
+                                              unsigned char* smem_raw)
 {
     static_assert(JB % 4 == 0 && JB <= 32, "panel width");
+    static_assert(NT % 32 == 0 && NT <= 1024, "CTA size");
     using K = typename KeyOf<T>::type;
     using SM = CtaLuSmem<T, NT, JB>;
     constexpr int NW = NT / 32;
@@ -334,32 +359,17 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                     crow[buf * NW + warp] = wr;
                 }
                 __syncthreads();
-                // every warp's record is read up front, then reduced: largest key,
-                // smallest position on ties (LAPACK: first index of the maximum)
-                K kw[NW];
-                int rw[NW];
-#pragma unroll
-                for(int w = 0; w < NW; ++w)
-                {
-                    kw[w] = ckey[buf * NW + w];
-                    rw[w] = w < nact ? crow[buf * NW + w] : INT_MAX;
-                }
-                K gk = kw[0];
-                int gr = rw[0];
-                gw = 0;
-#pragma unroll
-                for(int w = 1; w < NW; ++w)
-                {
-                    const bool better = rw[w] != INT_MAX
-                                        && (gr == INT_MAX || kw[w] > gk
-                                            || (kw[w] == gk && rw[w] < gr));
-                    if(better)
-                    {
-                        gk = kw[w];
-                        gr = rw[w];
-                        gw = w;
-                    }
-                }
+                // the warps' records are reduced lane-parallel (lane w holds warp w's
+                // record): largest key, smallest position on ties (LAPACK: first index of
+                // the maximum); gw = the warp that published the winning row
+                const bool rv = lane < nact;
+                const K kl = rv ? ckey[buf * NW + lane] : K(0);
+                const int rl = rv ? crow[buf * NW + lane] : INT_MAX;
+                K gk;
+                const int gr = warp_argmax(kl, rl, rv && rl != INT_MAX, &gk);
+                gw = __ffs(__ballot_sync(0xffffffffu, rv && rl == gr && kl == gk)) - 1;
+                if(gw < 0)
+                    gw = 0;
                 prow = gr;
             }
             else
@@ -476,9 +486,11 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             for(int i = 0; i < 32; ++i)
                 sLi[lane * SM::LDI + i] = x[i];
         }
-        // ---------------- row interchanges on the other columns: warp-local per column
+        // ---------------- row interchanges: warp-local gather/scatter of the moved rows, 4
+        // columns per batch, on the columns left of the panel (finished L) and, unless they
+        // are folded into the trailing update, on the columns right of it
         const int nm = PIVOT ? *nmoved : 0;
-        const int nother = n - jb;
+        const int nother = fold ? j0 : n - jb;
         if(nm > 0)
         {
             for(int o0 = warp * 4; o0 < nother; o0 += NW * 4)
@@ -514,20 +526,31 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             }
         }
         __syncthreads();
-        // ---------------- trailing update, column chunk by column chunk
+        // ---------------- trailing update, column chunk by column chunk.  With fold, the
+        // panel's row interchanges are applied here: position p of the chunk receives the
+        // original row slotof[p].  A position below the panel rows (p >= jb) either keeps
+        // its row or receives an original top row (p < jb): a row only moves down when it
+        // sits in the position of the column being pivoted, and only top positions are
+        // pivoted.  So:
+        //   1. stage A12 from the sources of the top positions (reads only, into sU);
+        //   2. U12 = L11^{-1} A12 in sU;
+        //   3. A22 tiles read position p from global row slotof[p] (itself or an untouched
+        //      top row) and write position p: no position is read after it is written;
+        //   4. U12 goes to the top rows last, once no tile needs their original values.
+        // Without fold the rows are already in place and U12 is stored as it is formed.
         const int mt = mp - jb;
         for(int c0 = j0 + jb; c0 < n; c0 += cw)
         {
             const int ncol = min(cw, n - c0);
             const int ncp = (ncol + 31) & ~31;
-            // stage A12 (rows j0..j0+jb-1 of the chunk), zero padded to JB x ncp
             for(int e = tid; e < JB * ncp; e += NT)
             {
                 const int k = e % JB, col = e / JB;
-                sU[k * cwp + col] = (k < jb && col < ncol) ? a[ix(j0 + k, c0 + col, lda)] : T(0);
+                sU[k * cwp + col] = (k < jb && col < ncol)
+                                        ? a[ix(j0 + (fold ? slotof[k] : k), c0 + col, lda)]
+                                        : T(0);
             }
             __syncthreads();
-            // U12 = L11^{-1} A12 in place, one 32-column tile per warp
             for(int t = warp; t < ncp / 32; t += NW)
             {
                 WarpTile<T> w;
@@ -542,12 +565,12 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                     const int col = t * 32 + cc;
                     if(rr < JB)
                         sU[rr * cwp + col] = rr < jb ? v : T(0);
-                    if(rr < jb && col < ncol)
+                    if(!fold && rr < jb && col < ncol)
                         a[ix(j0 + rr, c0 + col, lda)] = v;
                 });
             }
             __syncthreads();
-            // A22 -= L21 U12: 32x32 tiles of (mt x ncol); A rows through the slot table
+            // A22 -= L21 U12: 32x32 tiles of (mt x ncol); L21 rows through the slot table
             const int tm = (mt + 31) / 32, tn = ncp / 32;
             for(int t = warp; t < tm * tn; t += NW)
             {
@@ -562,7 +585,9 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                 }
                 w.each([&](int rr, int cc, T& v) {
                     const int r = r0 + rr, col = cc0 + cc;
-                    v = (r < mt && col < ncol) ? a[ix(j0 + jb + r, c0 + col, lda)] : T(0);
+                    v = (r < mt && col < ncol)
+                            ? a[ix(j0 + (fold ? slotof[jb + r] : jb + r), c0 + col, lda)]
+                            : T(0);
                 });
                 w.template mma<JB>(sP, ldp, arow, sU, cwp, cc0);
                 w.each([&](int rr, int cc, T& v) {
@@ -572,6 +597,16 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                 });
             }
             __syncthreads();
+            if(fold)
+            {
+                for(int e = tid; e < JB * ncol; e += NT)
+                {
+                    const int k = e % JB, col = e / JB;
+                    if(k < jb)
+                        a[ix(j0 + k, c0 + col, lda)] = sU[k * cwp + col];
+                }
+                __syncthreads();
+            }
         }
     }
     if(tid == 0)
@@ -579,16 +614,16 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
 }
 
 template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
-__global__ void __launch_bounds__(NT, LU_MIN_BLOCKS)
+__global__ void __launch_bounds__(NT, NT <= 128 ? 3 : LU_MIN_BLOCKS)
     getrf_cta_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
-                     int cw, Gate gate)
+                     int cw, int fold, Gate gate)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int64_t b = blockIdx.x;
     if(gate.skip(b))
         return;
     getrf_cta_dev<T, NT, R, JB, TN, PIVOT>(m, n, A.at(b), lda, PIVOT ? ipiv + b * strideP : nullptr,
-                                           info + b, cw, smem_raw);
+                                           info + b, cw, fold != 0, smem_raw);
 }
 
 } // namespace rsb

@@ -12,7 +12,7 @@
 // cte = ||A||_inf * eps * sqrt(n), eps = 2^-53.
 //
 // Pipeline (all on the handle's stream, no host synchronisation):
-//   1. convert : A -> FP32 copy in the workspace, ||A||_inf, overflow flags, info = iter = 0
+//   1. convert : A -> FP32 copy in the workspace, overflow flags, info = iter = 0
 //   2. sgetrf  : FP32 LU of the copy (same kernels as getrf, FP32 instantiation)
 //   3. refine  : one CTA per matrix: x = LU32^{-1} b, then r = b - A x in FP64 (A read in
 //                FP64), d = LU32^{-1} r in FP32, x += d, until the stopping rule holds
@@ -29,12 +29,19 @@ constexpr int DSGESV_ITERMAX = 10;
 // refinement solves use inverted diagonal blocks up to this order (their shared memory
 // grows as n); larger orders use the staged-block substitution
 constexpr int REFINE_BLOCKINV_MAXN = 512;
+// CTAs of the refinement kernel resident per SM: their A (FP64) and FP32 factors should
+// stay in L2 between iterations
+#ifndef REFINE_CTAS_PER_SM
+#define REFINE_CTAS_PER_SM 2
+#endif
 
+// A -> FP32 copy (ld n), FP32 overflow flag (LAPACK dsgesv: any |a_ij| > FLT_MAX sends
+// the member to the FP64 path), info = iter = 0.  One CTA per matrix, threads over rows,
+// 8 columns of loads in flight per thread.
 __global__ void __launch_bounds__(256)
-    dsgesv_convert_kernel(int n, Batch<double> A, int lda, float* a32, double* anrm, int* flag,
-                          int* info, int* iter)
+    dsgesv_convert_kernel(int n, Batch<double> A, int lda, float* a32, int* flag, int* info,
+                          int* iter)
 {
-    __shared__ double red[8];
     __shared__ int ovf;
     const int64_t b = blockIdx.x;
     const double* a = A.at(b);
@@ -42,33 +49,35 @@ __global__ void __launch_bounds__(256)
     if(threadIdx.x == 0)
         ovf = 0;
     __syncthreads();
-    double rmax = 0.0;
     int ov = 0;
     for(int i = threadIdx.x; i < n; i += blockDim.x)
     {
-        double rs = 0.0;
-        for(int j = 0; j < n; ++j)
+        int j = 0;
+        for(; j + 8 <= n; j += 8)
+        {
+            double v[8];
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
+                v[u] = a[ix(i, j + u, lda)];
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
+            {
+                ov |= fabs(v[u]) > (double)FLT_MAX;
+                s[ix(i, j + u, n)] = (float)v[u];
+            }
+        }
+        for(; j < n; ++j)
         {
             const double v = a[ix(i, j, lda)];
-            ov |= (v > (double)FLT_MAX || v < -(double)FLT_MAX);
+            ov |= fabs(v) > (double)FLT_MAX;
             s[ix(i, j, n)] = (float)v;
-            rs += fabs(v);
         }
-        rmax = fmax(rmax, rs);
     }
-    for(int o = 16; o > 0; o >>= 1)
-        rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-    if((threadIdx.x & 31) == 0)
-        red[threadIdx.x >> 5] = rmax;
     if(ov)
         atomicOr(&ovf, 1);
     __syncthreads();
     if(threadIdx.x == 0)
     {
-        double m = 0.0;
-        for(int w = 0; w < (int)(blockDim.x >> 5); ++w)
-            m = fmax(m, red[w]);
-        anrm[b] = m;
         flag[b] = ovf;
         info[b] = 0;
         iter[b] = 0;
@@ -111,18 +120,23 @@ __device__ void invert_diag_blocks(const float* lu, int n, float* sinv)
         const bool upper = t >= nblk;
         const int kb = (upper ? t - nblk : t) * 32, nb = min(32, n - kb);
         float* blk = sinv + t * BI_ELEMS;
-#pragma unroll 4
-        for(int k = 0; k < 32; ++k)
         {
+            // all 32 loads of the block column strip in flight before the stores
             const int i = lane;
-            float v;
-            if(i >= nb || k >= nb)
-                v = i == k ? 1.f : 0.f;
-            else if(!upper)
-                v = i > k ? lu[(kb + i) + (size_t)(kb + k) * n] : (i == k ? 1.f : 0.f);
-            else
-                v = i <= k ? lu[(kb + i) + (size_t)(kb + k) * n] : 0.f;
-            blk[i * BI_LD + k] = v;
+            float v[32];
+#pragma unroll
+            for(int k = 0; k < 32; ++k)
+            {
+                if(i >= nb || k >= nb)
+                    v[k] = i == k ? 1.f : 0.f;
+                else if(!upper)
+                    v[k] = i > k ? lu[(kb + i) + (size_t)(kb + k) * n] : (i == k ? 1.f : 0.f);
+                else
+                    v[k] = i <= k ? lu[(kb + i) + (size_t)(kb + k) * n] : 0.f;
+            }
+#pragma unroll
+            for(int k = 0; k < 32; ++k)
+                blk[i * BI_LD + k] = v[k];
         }
         __syncwarp();
         float x[32];
@@ -231,12 +245,154 @@ __device__ void blockinv_sweep(bool forward, const float* lu, int n, const float
     }
 }
 
+// blockinv_sweep for n <= NT with a fixed row per thread (row = threadIdx.x), so that the
+// factor strip a thread needs for block bi+1 can be loaded as soon as block bi's update has
+// consumed the previous one: the loads overlap the barrier and the next diagonal-block
+// product instead of following them.
 template <int NT, int NRC>
-__global__ void __launch_bounds__(NT)
+__device__ void blockinv_sweep_pf(bool forward, const float* lu, int n, const float* sinv,
+                                  float* s, int nc)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nblk = (n + 31) / 32;
+    const int i = tid;
+    float mv[32];
+    {
+        const int kb = forward ? 0 : (nblk - 1) * 32, nb = min(32, n - kb);
+        const bool act = forward ? (i >= kb + nb && i < n) : (i < kb);
+        if(act)
+        {
+#pragma unroll
+            for(int k = 0; k < 32; ++k)
+                mv[k] = k < nb ? lu[i + (size_t)(kb + k) * n] : 0.f;
+        }
+    }
+    for(int bi = 0; bi < nblk; ++bi)
+    {
+        const int blkid = forward ? bi : nblk - 1 - bi;
+        const int kb = blkid * 32, nb = min(32, n - kb);
+        const float* inv = sinv + (forward ? blkid : nblk + blkid) * BI_ELEMS;
+        if(warp == 0)
+        {
+            float y0[NRC], y1[NRC];
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                y0[c] = y1[c] = 0.f;
+#pragma unroll 4
+            for(int j = 0; j < 32; j += 2)
+            {
+                const float m0 = inv[lane * BI_LD + j], m1 = inv[lane * BI_LD + j + 1];
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                    if(c < nc)
+                    {
+                        if(j < nb)
+                            y0[c] = fmaf(m0, s[kb + j + c * n], y0[c]);
+                        if(j + 1 < nb)
+                            y1[c] = fmaf(m1, s[kb + j + 1 + c * n], y1[c]);
+                    }
+            }
+            __syncwarp();
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                if(c < nc && lane < nb)
+                    s[kb + lane + c * n] = y0[c] + y1[c];
+        }
+        __syncthreads();
+        const bool act = forward ? (i >= kb + nb && i < n) : (i < kb);
+        if(act)
+        {
+            float acc[NRC];
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                acc[c] = c < nc ? s[i + c * n] : 0.f;
+#pragma unroll
+            for(int k = 0; k < 32; ++k)
+                if(k < nb)
+#pragma unroll
+                    for(int c = 0; c < NRC; ++c)
+                        acc[c] = fmaf(-mv[k], s[kb + k + c * n], acc[c]);
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                if(c < nc)
+                    s[i + c * n] = acc[c];
+        }
+        // the next block's strip (its rows are a subset of this block's, or the same)
+        if(bi + 1 < nblk)
+        {
+            const int kb2 = forward ? kb + 32 : kb - 32, nb2 = min(32, n - kb2);
+            const bool act2 = forward ? (i >= kb2 + nb2 && i < n) : (i < kb2);
+            if(act2)
+            {
+#pragma unroll
+                for(int k = 0; k < 32; ++k)
+                    mv[k] = k < nb2 ? lu[i + (size_t)(kb2 + k) * n] : 0.f;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// r = b - A x for right-hand sides c0..c0+nc-1 in FP64, threads over rows (column-major A:
+// a warp reads 32 consecutive rows of a column), 8 columns of loads in flight per thread.
+// With rowsum, also returns this thread's largest row sum of |A| (for ||A||_inf).
+template <int NT, int NRC>
+__device__ double residual_rows(const double* a, int lda, const double* bb, int ldb,
+                                const double* xs, double* rs, int n, int c0, int nc,
+                                bool rowsum)
+{
+    double amax = 0.0;
+    for(int i = threadIdx.x; i < n; i += NT)
+    {
+        double acc[NRC];
+#pragma unroll
+        for(int c = 0; c < NRC; ++c)
+            acc[c] = c < nc ? bb[ix(i, c0 + c, ldb)] : 0.0;
+        double asum = 0.0;
+        int j = 0;
+#pragma unroll 2
+        for(; j + 8 <= n; j += 8)
+        {
+            double v[8];
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
+                v[u] = a[ix(i, j + u, lda)];
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
+            {
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                    if(c < nc)
+                        acc[c] = fma(-v[u], xs[j + u + (size_t)(c0 + c) * n], acc[c]);
+                if(rowsum)
+                    asum += fabs(v[u]);
+            }
+        }
+        for(; j < n; ++j)
+        {
+            const double v = a[ix(i, j, lda)];
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                if(c < nc)
+                    acc[c] = fma(-v, xs[j + (size_t)(c0 + c) * n], acc[c]);
+            if(rowsum)
+                asum += fabs(v);
+        }
+#pragma unroll
+        for(int c = 0; c < NRC; ++c)
+            if(c < nc)
+                rs[i + (size_t)(c0 + c) * n] = acc[c];
+        amax = fmax(amax, asum);
+    }
+    return amax;
+}
+
+template <int NT, int NRC>
+__global__ void __launch_bounds__(NT, REFINE_CTAS_PER_SM)
     dsgesv_refine_kernel(int n, int nrhs, Batch<double> A, int lda, const float* lu32,
                          const int* ipiv, int64_t strideP, Batch<double> B, int ldb,
-                         Batch<double> X, int ldx, const double* anrm, int* flag,
-                         const int* info32, int* iter, int itermax)
+                         Batch<double> X, int ldx, int* flag, const int* info32, int* iter,
+                         int itermax)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* xs = reinterpret_cast<double*>(smem_raw);   // n x nrhs
@@ -265,13 +421,9 @@ __global__ void __launch_bounds__(NT)
     const double* bb = B.at(b);
     double* x = X.at(b);
     const float* lu = lu32 + (size_t)b * n * n;
-    build_perm(ipiv + b * strideP, n, perm);
     if(blockinv)
-    {
         invert_diag_blocks<NT>(lu, n, sinv);
-        __syncthreads();
-    }
-    const double cte = anrm[b] * (DBL_EPSILON * 0.5) * sqrt((double)n);
+    build_perm(ipiv + b * strideP, n, perm);
     const int tot = n * nrhs;
     for(int e = tid; e < tot; e += NT)
     {
@@ -282,6 +434,7 @@ __global__ void __launch_bounds__(NT)
     if(tid == 0)
         bad = 0;
     __syncthreads();
+    double cte = 0.0;
     for(int it = 0;; ++it)
     {
         // ---- correction d = (LU32)^{-1} P r in FP32, x += d
@@ -297,7 +450,12 @@ __global__ void __launch_bounds__(NT)
                 s32[i + c * n] = (float)v;
             }
             __syncthreads();
-            if(blockinv)
+            if(blockinv && n <= NT)
+            {
+                blockinv_sweep_pf<NT, NRC>(true, lu, n, sinv, s32, nc);
+                blockinv_sweep_pf<NT, NRC>(false, lu, n, sinv, s32, nc);
+            }
+            else if(blockinv)
             {
                 blockinv_sweep<NT, NRC>(true, lu, n, sinv, s32, nc);
                 blockinv_sweep<NT, NRC>(false, lu, n, sinv, s32, nc);
@@ -325,30 +483,15 @@ __global__ void __launch_bounds__(NT)
             }
             return;
         }
-        // ---- residual r = b - A x in FP64 (column-major A: threads over rows coalesce)
-        for(int i = tid; i < n; i += NT)
-        {
-            for(int c = 0; c < nrhs; ++c)
-            {
-                double acc = bb[ix(i, c, ldb)];
-                const double* xc = xs + (size_t)c * n;
-                int j = 0;
-                for(; j + 4 <= n; j += 4)
-                {
-                    const double a0 = a[ix(i, j, lda)], a1 = a[ix(i, j + 1, lda)];
-                    const double a2 = a[ix(i, j + 2, lda)], a3 = a[ix(i, j + 3, lda)];
-                    acc = fma(-a0, xc[j], acc);
-                    acc = fma(-a1, xc[j + 1], acc);
-                    acc = fma(-a2, xc[j + 2], acc);
-                    acc = fma(-a3, xc[j + 3], acc);
-                }
-                for(; j < n; ++j)
-                    acc = fma(-a[ix(i, j, lda)], xc[j], acc);
-                rs[i + c * n] = acc;
-            }
-        }
+        // ---- residual r = b - A x in FP64; the first pass also yields ||A||_inf
+        double amax = 0.0;
+        for(int c0 = 0; c0 < nrhs; c0 += NRC)
+            amax = fmax(amax, residual_rows<NT, NRC>(a, lda, bb, ldb, xs, rs, n, c0,
+                                                    min(NRC, nrhs - c0), it == 0 && c0 == 0));
+        if(it == 0)
+            cte = block_max<NT>(amax, red) * (DBL_EPSILON * 0.5) * sqrt((double)n);
         __syncthreads();
-        // ---- stopping rule, every column
+        // ---- stopping rule (LAPACK dsgesv): every column, ||r||_inf <= ||x||_inf * cte
         bool conv = true;
         for(int c = 0; c < nrhs; ++c)
         {
@@ -426,8 +569,7 @@ static size_t refine_smem(int n, int nrhs, int NRC, int NT)
 size_t dsgesv_workspace(int n, int nrhs, int bc)
 {
     (void)nrhs;
-    return ws_round(sizeof(float) * (size_t)n * n * bc) + ws_round(sizeof(double) * bc)
-           + 3 * ws_round(sizeof(int) * bc);
+    return ws_round(sizeof(float) * (size_t)n * n * bc) + 3 * ws_round(sizeof(int) * bc);
 }
 
 rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, int lda,
@@ -437,8 +579,6 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
     char* p = static_cast<char*>(ws);
     float* a32 = reinterpret_cast<float*>(p);
     p += ws_round(sizeof(float) * (size_t)n * n * bc);
-    double* anrm = reinterpret_cast<double*>(p);
-    p += ws_round(sizeof(double) * bc);
     int* flag = reinterpret_cast<int*>(p);
     p += ws_round(sizeof(int) * bc);
     int* info32 = reinterpret_cast<int*>(p);
@@ -449,7 +589,7 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
     const bool refine_ok = smem <= 200 * 1024 && n <= MAX_CTA_ROWS;
     if(refine_ok)
     {
-        dsgesv_convert_kernel<<<bc, 256, 0, s>>>(n, A, lda, a32, anrm, flag, info, iter);
+        dsgesv_convert_kernel<<<bc, 256, 0, s>>>(n, A, lda, a32, flag, info, iter);
         if(cudaGetLastError() != cudaSuccess)
             return rocblas_status_internal_error;
         rocblas_status st = launch_getrf<float>(s, n, n, strided<float>(a32, (int64_t)n * n), n,
@@ -463,7 +603,7 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
                                     (int)smem)
                != cudaSuccess)
                 return rocblas_status_internal_error;
-            k<<<bc, NT, smem, s>>>(n, nrhs, A, lda, a32, ipiv, strideP, B, ldb, X, ldx, anrm, flag,
+            k<<<bc, NT, smem, s>>>(n, nrhs, A, lda, a32, ipiv, strideP, B, ldb, X, ldx, flag,
                                    info32, iter, DSGESV_ITERMAX);
         }
         else
@@ -473,7 +613,7 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
                                     (int)smem)
                != cudaSuccess)
                 return rocblas_status_internal_error;
-            k<<<bc, NT, smem, s>>>(n, nrhs, A, lda, a32, ipiv, strideP, B, ldb, X, ldx, anrm, flag,
+            k<<<bc, NT, smem, s>>>(n, nrhs, A, lda, a32, ipiv, strideP, B, ldb, X, ldx, flag,
                                    info32, iter, DSGESV_ITERMAX);
         }
         if(cudaGetLastError() != cudaSuccess)

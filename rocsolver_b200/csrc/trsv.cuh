@@ -152,10 +152,55 @@ __device__ void block_sweep(bool forward, bool unit, TriView<T> M, int n, T* sb,
 }
 
 // Source map of LAPACK dlaswp(k1=1, k2=n, incx=1): position i receives original row
-// perm[i].  Serial in the swap order (each interchange depends on the previous ones).
+// perm[i].  Applying interchange k to an array maps a'[i] = a[f_k(i)] with f_k the
+// transposition (k, piv[k]-1), so after all n interchanges perm[i] = f_0(f_1(...f_{n-1}(i))).
+// For n <= 2*blockDim.x every thread evaluates that composition for its own positions
+// (k from n-1 down to 0, pivots staged in shared memory and read as broadcasts): no
+// serial chain through memory.
+// Larger n replays the interchanges serially in one thread.  A pivot outside [1, n] never
+// yields an index outside the matrix.
 __device__ __forceinline__ void build_perm(const int* piv, int n, int* perm)
 {
-    for(int i = threadIdx.x; i < n; i += blockDim.x)
+    const int nt = blockDim.x;
+    if(n <= 2 * nt)
+    {
+        // pivots staged in perm[] (one coalesced load), read back as broadcasts
+        for(int k = threadIdx.x; k < n; k += nt)
+            perm[k] = piv[k] - 1;
+        __syncthreads();
+        const int i0 = threadIdx.x, i1 = threadIdx.x + nt;
+        int x0 = i0, x1 = i1;
+        int k = n - 1;
+        for(; k >= 7; k -= 8)
+        {
+            int p[8];
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
+                p[u] = perm[k - u];
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
+            {
+                const int kk = k - u;
+                x0 = x0 == kk ? p[u] : (x0 == p[u] ? kk : x0);
+                x1 = x1 == kk ? p[u] : (x1 == p[u] ? kk : x1);
+            }
+        }
+        for(; k >= 0; --k)
+        {
+            const int p = perm[k];
+            x0 = x0 == k ? p : (x0 == p ? k : x0);
+            x1 = x1 == k ? p : (x1 == p ? k : x1);
+        }
+        __syncthreads();
+        // an out-of-range pivot can only have produced an out-of-range x: keep the row
+        if(i0 < n)
+            perm[i0] = (x0 >= 0 && x0 < n) ? x0 : i0;
+        if(i1 < n)
+            perm[i1] = (x1 >= 0 && x1 < n) ? x1 : i1;
+        __syncthreads();
+        return;
+    }
+    for(int i = threadIdx.x; i < n; i += nt)
         perm[i] = i;
     __syncthreads();
     if(threadIdx.x == 0)
@@ -163,7 +208,7 @@ __device__ __forceinline__ void build_perm(const int* piv, int n, int* perm)
         for(int k = 0; k < n; ++k)
         {
             const int p = piv[k] - 1;
-            if(p != k)
+            if(p != k && p >= 0 && p < n)
             {
                 const int t = perm[k];
                 perm[k] = perm[p];
@@ -217,7 +262,7 @@ __device__ __forceinline__ void getrs_dev(int trans, int n, int nrhs, const T* a
 // trans != 0: U' forward, L' (unit) backward, P' x.
 // (library/src/lapack/roclapack_getrs.hpp:117-150)
 template <typename T, int NT, int NRC>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
     getrs_cta_kernel(int trans, int n, int nrhs, Batch<T> A, int lda, const int* ipiv,
                      int64_t strideP, Batch<T> B, int ldb, const int* skip_info, Gate gate)
 {
@@ -264,7 +309,7 @@ __global__ void __launch_bounds__(NT)
 // potrs for any n: A = L L' (lower) or U' U (upper)
 // (library/src/lapack/roclapack_potrs.hpp:87-152).
 template <typename T, int NT, int NRC>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
     potrs_cta_kernel(int upper, int n, int nrhs, Batch<T> A, int lda, Batch<T> B, int ldb,
                      const int* skip_info)
 {

@@ -15,6 +15,7 @@
 // (solve) ldb < n / nrhs < 0 / nrhs > max_nrhs gets info = -1 and is left untouched.
 #include "handle.h"
 #include "launch.h"
+#include "tuning.h"
 #include "lu_cta.cuh"
 #include "lu_small.cuh"
 #include "trsv.cuh"
@@ -90,8 +91,8 @@ __device__ __forceinline__ bool vb_valid(const VbArgs& v, int b)
 }
 
 template <typename T, int NT, int R, int JB, int TN>
-__global__ void __launch_bounds__(NT)
-    vb_persistent_kernel(VbArgs v, T* const* A, T* const* B, int cw)
+__global__ void __launch_bounds__(NT, 2)
+    vb_persistent_kernel(VbArgs v, T* const* A, T* const* B, int cw, int fold)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ T srow[VB_WARPS][2][32];
@@ -119,8 +120,13 @@ __global__ void __launch_bounds__(NT)
         const int n = v.n[b];
         if(v.mode != 2)
         {
-            getrf_cta_dev<T, NT, R, JB, TN, true>(n, n, A[b], v.lda[b], v.ipiv[b], v.info + b, cw,
-                                                  smem_raw);
+            // members up to 256 use the one-row-per-thread, 32-wide-panel configuration
+            if(R > 1 && n <= NT)
+                getrf_cta_dev<T, NT, 1, 32, TN, true>(n, n, A[b], v.lda[b], v.ipiv[b],
+                                                      v.info + b, cw, fold != 0, smem_raw);
+            else
+                getrf_cta_dev<T, NT, R, JB, TN, true>(n, n, A[b], v.lda[b], v.ipiv[b],
+                                                      v.info + b, cw, fold != 0, smem_raw);
             __syncthreads();
         }
         if(v.mode != 1 && (v.mode == 2 || v.info[b] == 0))
@@ -222,18 +228,37 @@ static int sm_count()
     return c;
 }
 
+// cw: trailing column chunk (0 = default), fold: interchange folding (see getrf_cta_dev),
+// per_sm: CTAs launched per SM (0 = as many as fit).  *ran = false when the configuration
+// cannot take this batch (too many rows, too much shared memory).
 template <typename T, int NT, int R, int JB, int TN>
-static rocblas_status run_vb(cudaStream_t s, VbArgs v, T* const* A, T* const* B)
+static rocblas_status run_vb(cudaStream_t s, VbArgs v, T* const* A, T* const* B, int cw,
+                             int fold, int per_sm_req, bool* ran = nullptr)
 {
+    if(ran)
+        *ran = false;
+    if(v.max_n > NT * R)
+        return rocblas_status_not_implemented;
     const int cwmax = sizeof(T) == 8 ? LU_CW_F64 : LU_CW_F32;
-    int cw = ((v.max_n + 31) / 32) * 32;
-    if(cw > cwmax)
+    const int nround = ((v.max_n + 31) / 32) * 32;
+    if(cw <= 0)
         cw = cwmax;
+    cw = ((cw + 31) / 32) * 32;
+    if(cw > nround)
+        cw = nround;
     size_t smem = CtaLuSmem<T, NT, JB>::bytes(v.max_n, cw, R);
+    if(R > 1)
+    {
+        const size_t s1 = CtaLuSmem<T, NT, 32>::bytes(NT, cw, 1);
+        if(s1 > smem)
+            smem = s1;
+    }
     const size_t solve = sizeof(T) * ((size_t)v.max_n * 4 + SDIAG_ELEMS)
                          + sizeof(int) * (size_t)v.max_n;
     if(solve > smem)
         smem = solve;
+    if(smem > 227 * 1024)
+        return rocblas_status_not_implemented;
     auto k = vb_persistent_kernel<T, NT, R, JB, TN>;
     if(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
        != cudaSuccess)
@@ -242,10 +267,14 @@ static rocblas_status run_vb(cudaStream_t s, VbArgs v, T* const* A, T* const* B)
     if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem) != cudaSuccess
        || per_sm < 1)
         per_sm = 1;
+    if(per_sm_req > 0 && per_sm_req < per_sm)
+        per_sm = per_sm_req;
     int grid = sm_count() * per_sm;
     if(grid > v.bc)
         grid = v.bc;
-    k<<<grid, NT, smem, s>>>(v, A, B, cw);
+    if(ran)
+        *ran = true;
+    k<<<grid, NT, smem, s>>>(v, A, B, cw, fold);
     return cudaGetLastError() == cudaSuccess ? rocblas_status_success
                                              : rocblas_status_internal_error;
 }
@@ -274,13 +303,29 @@ rocblas_status launch_vbatched(cudaStream_t s, int mode, const int* n, const int
     vb_plan_kernel<<<1, 1024, sizeof(int) * (max_n + 2), s>>>(v);
     if(cudaGetLastError() != cudaSuccess)
         return rocblas_status_internal_error;
+    VbCfg c;
+    if(tuned_vbatched(sizeof(T) == 8 ? 'd' : 's', max_n, &c) && c.nt == 256)
+    {
+        bool ran = false;
+        rocblas_status st = rocblas_status_not_implemented;
+        if(c.r == 1 && c.jb == 32)
+            st = run_vb<T, 256, 1, 32, 8>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
+        else if(c.r == 2 && c.jb == 16)
+            st = run_vb<T, 256, 2, 16, 8>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
+        else if(c.r == 4 && c.jb == 8)
+            st = run_vb<T, 256, 4, 8, 4>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
+        else if(c.r == 8 && c.jb == 4)
+            st = run_vb<T, 256, 8, 4, 4>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
+        if(ran)
+            return st;
+    }
     if(max_n <= 256)
-        return run_vb<T, 256, 1, 32, 8>(s, v, A, B);
+        return run_vb<T, 256, 1, 32, 8>(s, v, A, B, 0, 0, 0);
     if(max_n <= 512)
-        return run_vb<T, 256, 2, 16, 8>(s, v, A, B);
+        return run_vb<T, 256, 2, 16, 8>(s, v, A, B, 0, 0, 0);
     if(max_n <= 1024)
-        return run_vb<T, 256, 4, 8, 4>(s, v, A, B);
-    return run_vb<T, 256, 8, 4, 4>(s, v, A, B);
+        return run_vb<T, 256, 4, 8, 4>(s, v, A, B, 0, 0, 0);
+    return run_vb<T, 256, 8, 4, 4>(s, v, A, B, 0, 0, 0);
 }
 
 template rocblas_status launch_vbatched<float>(cudaStream_t, int, const int*, const int*,

@@ -14,6 +14,20 @@ import torch
 import rocsolver_b200 as rs
 
 
+def cond_matrices(torch, n, bc, g, dev, lo, hi):
+    """A = U diag(s) V' (U, V from QR of Gaussians), s log-spaced from 1 to 1/kappa,
+    log10(kappa) uniform in [lo, hi] per member."""
+    A = torch.empty(bc, n, n, dtype=torch.float64, device=dev)
+    t = torch.linspace(0, 1, n, device=dev, dtype=torch.float64)[None, :]
+    for c0 in range(0, bc, 256):
+        m = min(bc, c0 + 256) - c0
+        U, _ = torch.linalg.qr(torch.randn(m, n, n, generator=g, device=dev, dtype=torch.float64))
+        V, _ = torch.linalg.qr(torch.randn(m, n, n, generator=g, device=dev, dtype=torch.float64))
+        lk = lo + (hi - lo) * torch.rand(m, 1, generator=g, device=dev, dtype=torch.float64)
+        A[c0:c0 + m] = (U * torch.pow(10.0, -lk * t)[:, None, :]) @ V.transpose(1, 2)
+    return A
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
@@ -24,6 +38,8 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--dtype", default="d", choices=["s", "d"])
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--cond", type=float, default=0.0,
+                    help="dsgesv: A = U diag(s) V' with log10(cond) uniform in [1, COND]")
     a = ap.parse_args()
     dt = torch.float64 if a.dtype == "d" else torch.float32
     dev = torch.device("cuda")
@@ -33,6 +49,8 @@ def main():
     A0 = torch.rand(bc, n, n, generator=g, device=dev, dtype=dt) * 2 - 1
     if a.case in ("potrf", "potrs"):
         A0 = A0 @ A0.transpose(1, 2) + n * torch.eye(n, device=dev, dtype=dt)
+    elif a.case == "dsgesv" and a.cond > 0:
+        A0 = cond_matrices(torch, n, bc, g, dev, 1.0, a.cond)
     elif a.case in ("dsgesv", "adjoint"):
         A0 = A0 + 4 * torch.eye(n, device=dev, dtype=dt)
     A0 = A0.transpose(1, 2).contiguous()
@@ -108,6 +126,9 @@ def main():
     h.close()
     print(f"{a.case} {a.dtype} n={n} batch={bc} nrhs={nrhs}: median {statistics.median(times):.4f} ms"
           f" over {a.reps} calls; info nonzero {int((info != 0).sum())}")
+    if a.case == "dsgesv":
+        vals, cnt = torch.unique(it, return_counts=True)
+        print("iter histogram:", dict(zip(vals.tolist(), cnt.tolist())))
 
 
 if __name__ == "__main__":
