@@ -34,6 +34,9 @@ namespace rsb {
 #ifndef LU_MIN_BLOCKS
 #define LU_MIN_BLOCKS 2
 #endif
+#ifndef LU_MIN_BLOCKS_128
+#define LU_MIN_BLOCKS_128 4
+#endif
 #ifndef LU_CW_F64
 #define LU_CW_F64 64
 #endif
@@ -613,8 +616,12 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
         *info_out = inf;
 }
 
+// 128-thread CTAs: 3 per SM, or LU_MIN_BLOCKS_128 when the panel fits the smaller register
+// budget (FP32, or one row per thread)
 template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
-__global__ void __launch_bounds__(NT, NT <= 128 ? 3 : LU_MIN_BLOCKS)
+__global__ void __launch_bounds__(NT,
+                                  NT <= 128 ? ((sizeof(T) == 4 || R == 1) ? LU_MIN_BLOCKS_128 : 3)
+                                            : LU_MIN_BLOCKS)
     getrf_cta_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
                      int cw, int fold, Gate gate)
 {

@@ -34,6 +34,11 @@ constexpr int REFINE_BLOCKINV_MAXN = 512;
 #ifndef REFINE_CTAS_PER_SM
 #define REFINE_CTAS_PER_SM 2
 #endif
+// threads per refinement CTA (rows of at most half this order use two threads per row in
+// the residual)
+#ifndef REFINE_NT
+#define REFINE_NT 256
+#endif
 
 // A -> FP32 copy (ld n), FP32 overflow flag (LAPACK dsgesv: any |a_ij| > FLT_MAX sends
 // the member to the FP64 path), info = iter = 0.  One CTA per matrix, threads over rows,
@@ -387,6 +392,78 @@ __device__ double residual_rows(const double* a, int lda, const double* bb, int 
     return amax;
 }
 
+// residual_rows with two threads per row (n <= NT/2): thread t takes row t mod NT/2 and
+// half t div NT/2 of the columns; the second half's partial sums meet the first's through
+// shared memory (part, n*NRC doubles).  Same arithmetic per half as residual_rows; the two
+// halves are added once at the end.
+template <int NT, int NRC>
+__device__ double residual_rows_split(const double* a, int lda, const double* bb, int ldb,
+                                      const double* xs, double* rs, double* part, int n,
+                                      int c0, int nc, bool rowsum)
+{
+    constexpr int H = NT / 2;
+    const int i = threadIdx.x % H, h = threadIdx.x / H;
+    const int half = (n + 1) / 2;
+    const int j0 = h ? half : 0, j1 = h ? n : half;
+    double acc[NRC];
+    double asum = 0.0;
+#pragma unroll
+    for(int c = 0; c < NRC; ++c)
+        acc[c] = 0.0;
+    if(i < n)
+    {
+        int j = j0;
+#pragma unroll 2
+        for(; j + 8 <= j1; j += 8)
+        {
+            double v[8];
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
+                v[u] = a[ix(i, j + u, lda)];
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
+            {
+#pragma unroll
+                for(int c = 0; c < NRC; ++c)
+                    if(c < nc)
+                        acc[c] = fma(-v[u], xs[j + u + (size_t)(c0 + c) * n], acc[c]);
+                if(rowsum)
+                    asum += fabs(v[u]);
+            }
+        }
+        for(; j < j1; ++j)
+        {
+            const double v = a[ix(i, j, lda)];
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                if(c < nc)
+                    acc[c] = fma(-v, xs[j + (size_t)(c0 + c) * n], acc[c]);
+            if(rowsum)
+                asum += fabs(v);
+        }
+        if(h)
+        {
+#pragma unroll
+            for(int c = 0; c < NRC; ++c)
+                if(c < nc)
+                    part[i + c * n] = acc[c];
+            part[(size_t)NRC * n + i] = asum;
+        }
+    }
+    __syncthreads();
+    double amax = 0.0;
+    if(!h && i < n)
+    {
+#pragma unroll
+        for(int c = 0; c < NRC; ++c)
+            if(c < nc)
+                rs[i + (size_t)(c0 + c) * n] = bb[ix(i, c0 + c, ldb)] + (acc[c] + part[i + c * n]);
+        amax = asum + part[(size_t)NRC * n + i];
+    }
+    __syncthreads();
+    return amax;
+}
+
 template <int NT, int NRC>
 __global__ void __launch_bounds__(NT, REFINE_CTAS_PER_SM)
     dsgesv_refine_kernel(int n, int nrhs, Batch<double> A, int lda, const float* lu32,
@@ -403,6 +480,11 @@ __global__ void __launch_bounds__(NT, REFINE_CTAS_PER_SM)
     int* perm = reinterpret_cast<int*>(s32 + (size_t)n * NRC);
     float* sinv = reinterpret_cast<float*>(perm + ((n + 3) & ~3)); // [2*nblk][32x33]
     const bool blockinv = n <= REFINE_BLOCKINV_MAXN;
+    double* part = reinterpret_cast<double*>(
+        (reinterpret_cast<uintptr_t>(sinv + (blockinv ? 2 * ((n + 31) / 32) * BI_ELEMS : 0))
+         + 15)
+        & ~uintptr_t(15)); // (NRC+1) x n doubles, split residual rows
+    const bool split = 2 * n <= NT;
     __shared__ int bad;
 
     const int64_t b = blockIdx.x;
@@ -486,8 +568,12 @@ __global__ void __launch_bounds__(NT, REFINE_CTAS_PER_SM)
         // ---- residual r = b - A x in FP64; the first pass also yields ||A||_inf
         double amax = 0.0;
         for(int c0 = 0; c0 < nrhs; c0 += NRC)
-            amax = fmax(amax, residual_rows<NT, NRC>(a, lda, bb, ldb, xs, rs, n, c0,
-                                                    min(NRC, nrhs - c0), it == 0 && c0 == 0));
+            amax = fmax(amax,
+                        split ? residual_rows_split<NT, NRC>(a, lda, bb, ldb, xs, rs, part, n, c0,
+                                                             min(NRC, nrhs - c0),
+                                                             it == 0 && c0 == 0)
+                              : residual_rows<NT, NRC>(a, lda, bb, ldb, xs, rs, n, c0,
+                                                       min(NRC, nrhs - c0), it == 0 && c0 == 0));
         if(it == 0)
             cte = block_max<NT>(amax, red) * (DBL_EPSILON * 0.5) * sqrt((double)n);
         __syncthreads();
@@ -561,9 +647,10 @@ static size_t refine_smem(int n, int nrhs, int NRC, int NT)
 {
     const size_t nblk = (n + 31) / 32;
     const size_t inv = n <= REFINE_BLOCKINV_MAXN ? 2 * nblk * BI_ELEMS : 0;
+    const size_t part = 2 * n <= NT ? (size_t)(NRC + 1) * n : 0;
     return sizeof(double) * (2 * (size_t)n * nrhs + NT / 32)
            + sizeof(float) * ((size_t)n * NRC + SDIAG_ELEMS + inv)
-           + sizeof(int) * (size_t)((n + 3) & ~3);
+           + sizeof(int) * (size_t)((n + 3) & ~3) + sizeof(double) * part + 16;
 }
 
 size_t dsgesv_workspace(int n, int nrhs, int bc)
@@ -583,7 +670,7 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
     p += ws_round(sizeof(int) * bc);
     int* info32 = reinterpret_cast<int*>(p);
 
-    constexpr int NT = 256;
+    constexpr int NT = REFINE_NT;
     const int NRC = nrhs == 1 ? 1 : 4;
     const size_t smem = refine_smem(n, nrhs, NRC, NT);
     const bool refine_ok = smem <= 200 * 1024 && n <= MAX_CTA_ROWS;
