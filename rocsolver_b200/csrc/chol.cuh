@@ -180,4 +180,96 @@ __global__ void __launch_bounds__(NT)
         info[b] = inf;
 }
 
+// ---------------------------------------------------------------------------------------
+// Small orders (n <= N, N = 32 or 64): one thread per row, the row's lower-triangle
+// entries in registers for the whole factorisation, one CTA barrier per column.
+// Rolled column loop: at step c, v[i] holds A(r, c + i) of this thread's row r, so the
+// active column is always v[0] and the rank-1 update writes column c+1+i into v[i].  At
+// step c every row r >= c publishes A(r, c) (already updated by steps < c) at slot r-c of
+// a double-buffered column vector, the diagonal row also publishes sqrt and 1/sqrt of its
+// pivot (computed before the barrier), and after ONE barrier each row r > c forms
+// l = A(r, c) / L(c, c), stores it, and updates
+//   A(r, c+1+i) -= (l / L(c, c)) * A(c+1+i, c),   i = 0 .. N-2,
+// reading the published column as aligned vectors.  Entries right of the diagonal are
+// updated too (never stored).  Each row stores its column-c entry as it is finalised.
+// A non-positive or NaN pivot at step c: columns < c are final, A(c, c) keeps the updated
+// value, the rest of the matrix is untouched and info = c + 1 (LAPACK dpotf2).
+template <typename T, int N>
+__global__ void __launch_bounds__(N, N <= 32 ? 16 : 6)
+    potrf_reg_kernel(int upper, int n, Batch<T> A, int lda, int* info)
+{
+    // published column (slot r - c); rows of N + 4 elements keep both buffers 16-byte
+    // aligned for the vector reads in FP32 and FP64
+    __shared__ __align__(16) T scol[2][N + 4];
+    __shared__ T sdiag[2][2];                  // sqrt(pivot), 1/sqrt(pivot)
+    const int r = threadIdx.x;
+    const int64_t b = blockIdx.x;
+    T* a = A.at(b);
+    const int64_t rs = upper ? lda : 1, cs = upper ? 1 : lda;
+    auto at = [&](int i, int j) -> T& { return a[(int64_t)i * rs + (int64_t)j * cs]; };
+    T v[N];
+#pragma unroll
+    for(int i = 0; i < N; ++i)
+        v[i] = (r < n && i <= r) ? at(r, i) : T(0);
+    int inf = 0;
+#pragma unroll 1
+    for(int c = 0; c < n; ++c)
+    {
+        const int buf = c & 1;
+        if(r == c)
+        {
+            const T d = v[0];
+            const bool ok = d > T(0);
+            const T sq = ok ? sqrt(d) : d;
+            sdiag[buf][0] = sq;
+            sdiag[buf][1] = ok ? T(1) / sq : T(0);
+            at(c, c) = sq; // LAPACK also stores a failing pivot as it was computed
+        }
+        else if(r > c && r < n)
+            scol[buf][r - c - 1] = v[0];
+        __syncthreads();
+        const T sq = sdiag[buf][0];
+        if(!(sq > T(0)))
+        {
+            inf = c + 1;
+            break;
+        }
+        const T rcp = sdiag[buf][1];
+        if(r > c && r < n)
+        {
+            const T l = v[0] * rcp;
+            at(r, c) = l;
+            const T lr = l * rcp;
+            const T* col = scol[buf];
+            if constexpr(sizeof(T) == 8)
+            {
+#pragma unroll
+                for(int i = 0; i < N; i += 2)
+                {
+                    const double2 t = *reinterpret_cast<const double2*>(col + i);
+                    if(i + 1 < N)
+                        v[i] = fma(-lr, t.x, v[i + 1]);
+                    if(i + 2 < N)
+                        v[i + 1] = fma(-lr, t.y, v[i + 2]);
+                }
+            }
+            else
+            {
+#pragma unroll
+                for(int i = 0; i < N; i += 4)
+                {
+                    const float4 t = *reinterpret_cast<const float4*>(col + i);
+                    const float e[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                    for(int u = 0; u < 4; ++u)
+                        if(i + u + 1 < N)
+                            v[i + u] = fmaf(-lr, e[u], v[i + u + 1]);
+                }
+            }
+        }
+    }
+    if(r == 0)
+        info[b] = inf;
+}
+
 } // namespace rsb

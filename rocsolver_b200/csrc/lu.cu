@@ -302,14 +302,22 @@ static rocblas_status run_potrf(cudaStream_t s, int upper, int n, Batch<T> A, in
     return launch_status();
 }
 
+template <typename T, int N>
+static rocblas_status run_potrf_reg(cudaStream_t s, int upper, int n, Batch<T> A, int lda,
+                                    int* info, int bc)
+{
+    potrf_reg_kernel<T, N><<<bc, N, 0, s>>>(upper, n, A, lda, info);
+    return launch_status();
+}
+
 template <typename T>
 rocblas_status launch_potrf(cudaStream_t s, int upper, int n, Batch<T> A, int lda, int* info,
                             int bc)
 {
     if(n <= 32)
-        return run_potrf<T, 32, 1, 32, 8>(s, upper, n, A, lda, info, bc);
+        return run_potrf_reg<T, 32>(s, upper, n, A, lda, info, bc);
     if(n <= 64)
-        return run_potrf<T, 64, 1, 32, 8>(s, upper, n, A, lda, info, bc);
+        return run_potrf_reg<T, 64>(s, upper, n, A, lda, info, bc);
     if(n <= 256)
         return run_potrf<T, 256, 1, 32, 8>(s, upper, n, A, lda, info, bc);
     if(n <= 512)
@@ -334,10 +342,24 @@ static rocblas_status run_potrs_nt(cudaStream_t s, int upper, int n, int nrhs, B
     return launch_status();
 }
 
+template <typename T, int N, int NRC>
+static rocblas_status run_potrs_small(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A,
+                                      int lda, Batch<T> B, int ldb, const int* skip, int bc)
+{
+    const int64_t groups = (nrhs + NRC - 1) / NRC;
+    potrs_small_kernel<T, N, NRC>
+        <<<(unsigned)(bc * groups), N, 0, s>>>(upper, n, nrhs, A, lda, B, ldb, skip);
+    return launch_status();
+}
+
 template <typename T, int NRC>
 static rocblas_status run_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A,
                                 int lda, Batch<T> B, int ldb, const int* skip, int bc)
 {
+    if(n <= 32)
+        return run_potrs_small<T, 32, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
+    if(n <= 64)
+        return run_potrs_small<T, 64, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
     if(n <= 64)
         return run_potrs_nt<T, 64, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
     if(n <= 128)

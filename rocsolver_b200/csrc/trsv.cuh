@@ -347,4 +347,97 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
     }
 }
 
+// potrs for n <= N (N = 32 or 64 threads, one row each): the factor's triangle is staged
+// in shared memory once (coalesced along its stored direction), each thread keeps its
+// row's NRC right-hand-side values in registers, and both sweeps take one barrier per
+// column: the row owning column c finalises its value (times the reciprocal of the
+// diagonal, computed once per row off the critical path) and publishes it in a
+// double-buffered slot; the rows still to be solved subtract their multiple of it.
+template <typename T, int N, int NRC>
+__global__ void __launch_bounds__(N, N <= 32 ? 16 : 8)
+    potrs_small_kernel(int upper, int n, int nrhs, Batch<T> A, int lda, Batch<T> B, int ldb,
+                       const int* skip_info)
+{
+    constexpr int LD = N + 1;
+    __shared__ T sL[N * LD]; // L(r, c) at sL[r + c*LD], lower triangle
+    __shared__ T sx[2][NRC];
+    const int r = threadIdx.x;
+    const int groups = (nrhs + NRC - 1) / NRC;
+    const int64_t b = blockIdx.x / groups;
+    const int c0 = (blockIdx.x % groups) * NRC;
+    const int nc = min(NRC, nrhs - c0);
+    if(skip_info && skip_info[b] != 0)
+        return;
+    const T* a = A.at(b);
+    T* x = B.at(b);
+    // L(i, j) = a[i + j*lda] (lower) or U(j, i) = a[j + i*lda] (upper); the fastest thread
+    // index runs along the stored column either way
+    for(int e = r; e < N * N; e += N)
+    {
+        const int p = e % N, q = e / N;
+        const int i = upper ? q : p, j = upper ? p : q; // L(i, j), i >= j
+        if(i < n && j <= i)
+            sL[i + j * LD] = upper ? a[ix(j, i, lda)] : a[ix(i, j, lda)];
+    }
+    T v[NRC];
+#pragma unroll
+    for(int k = 0; k < NRC; ++k)
+        v[k] = (r < n && k < nc) ? x[ix(r, c0 + k, ldb)] : T(0);
+    __syncthreads();
+    const T rd = r < n ? T(1) / sL[r + r * LD] : T(0);
+    // forward: L y = b
+#pragma unroll 1
+    for(int c = 0; c < n; ++c)
+    {
+        const int buf = c & 1;
+        if(r == c)
+        {
+#pragma unroll
+            for(int k = 0; k < NRC; ++k)
+            {
+                v[k] *= rd;
+                sx[buf][k] = v[k];
+            }
+        }
+        __syncthreads();
+        if(r > c && r < n)
+        {
+            const T l = sL[r + c * LD];
+#pragma unroll
+            for(int k = 0; k < NRC; ++k)
+                v[k] = fma(-l, sx[buf][k], v[k]);
+        }
+    }
+    // backward: L' x = y
+#pragma unroll 1
+    for(int c = n - 1; c >= 0; --c)
+    {
+        const int buf = (c + 1) & 1; // step n-1 takes the buffer the forward sweep did not end on
+        if(r == c)
+        {
+#pragma unroll
+            for(int k = 0; k < NRC; ++k)
+            {
+                v[k] *= rd;
+                sx[buf][k] = v[k];
+            }
+        }
+        __syncthreads();
+        if(r < c)
+        {
+            const T l = sL[c + r * LD];
+#pragma unroll
+            for(int k = 0; k < NRC; ++k)
+                v[k] = fma(-l, sx[buf][k], v[k]);
+        }
+    }
+    if(r < n)
+    {
+#pragma unroll
+        for(int k = 0; k < NRC; ++k)
+            if(k < nc)
+                x[ix(r, c0 + k, ldb)] = v[k];
+    }
+}
+
 } // namespace rsb
