@@ -191,7 +191,8 @@ __global__ void __launch_bounds__(NT)
 // l = A(r, c) / L(c, c), stores it, and updates
 //   A(r, c+1+i) -= (l / L(c, c)) * A(c+1+i, c),   i = 0 .. N-2,
 // reading the published column as aligned vectors.  Entries right of the diagonal are
-// updated too (never stored).  Each row stores its column-c entry as it is finalised.
+// updated too (never stored) up to the warp's last row; beyond it they are skipped in
+// groups of 8.  Each row stores its column-c entry as it is finalised.
 // A non-positive or NaN pivot at step c: columns < c are final, A(c, c) keeps the updated
 // value, the rest of the matrix is untouched and info = c + 1 (LAPACK dpotf2).
 template <typename T, int N>
@@ -241,29 +242,38 @@ __global__ void __launch_bounds__(N, N <= 32 ? 16 : 6)
             at(r, c) = l;
             const T lr = l * rcp;
             const T* col = scol[buf];
-            if constexpr(sizeof(T) == 8)
-            {
+            // only columns up to the warp's last row matter: groups of 8 registers above
+            // that are skipped (the branch is uniform across the warp)
+            const int lim = min(32 * (r >> 5) + 31, n - 1) - c - 1;
 #pragma unroll
-                for(int i = 0; i < N; i += 2)
+            for(int g = 0; g < N; g += 8)
+            {
+                if(g > lim)
+                    break;
+                if constexpr(sizeof(T) == 8)
                 {
-                    const double2 t = *reinterpret_cast<const double2*>(col + i);
-                    if(i + 1 < N)
-                        v[i] = fma(-lr, t.x, v[i + 1]);
-                    if(i + 2 < N)
-                        v[i + 1] = fma(-lr, t.y, v[i + 2]);
+#pragma unroll
+                    for(int i = g; i < g + 8; i += 2)
+                    {
+                        const double2 t = *reinterpret_cast<const double2*>(col + i);
+                        if(i + 1 < N)
+                            v[i] = fma(-lr, t.x, v[i + 1]);
+                        if(i + 2 < N)
+                            v[i + 1] = fma(-lr, t.y, v[i + 2]);
+                    }
                 }
-            }
-            else
-            {
-#pragma unroll
-                for(int i = 0; i < N; i += 4)
+                else
                 {
-                    const float4 t = *reinterpret_cast<const float4*>(col + i);
-                    const float e[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
-                    for(int u = 0; u < 4; ++u)
-                        if(i + u + 1 < N)
-                            v[i + u] = fmaf(-lr, e[u], v[i + u + 1]);
+                    for(int i = g; i < g + 8; i += 4)
+                    {
+                        const float4 t = *reinterpret_cast<const float4*>(col + i);
+                        const float e[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                        for(int u = 0; u < 4; ++u)
+                            if(i + u + 1 < N)
+                                v[i + u] = fmaf(-lr, e[u], v[i + u + 1]);
+                    }
                 }
             }
         }

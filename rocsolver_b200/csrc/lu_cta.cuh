@@ -93,33 +93,42 @@ __device__ __forceinline__ void store_row_shifted(T* dst, const T (&v)[JB])
                 make_float4(at(i + 1), at(i + 2), at(i + 3), at(i + 4));
     }
 }
-// v[i] = fma(-l, row[i], v[i+1]) for i < JB-1 with row read as aligned vectors
+// v[i] = fma(-l, row[i], v[i+1]) for i <= lim (and i < JB-1) with row read as aligned
+// vectors.  Registers above lim hold columns outside the panel; they are left stale, in
+// groups of 8 skipped by a branch that is uniform across the CTA (lim depends only on
+// the column).
 template <typename T, int JB>
-__device__ __forceinline__ void update_shift(T (&v)[JB], T l, const T* row)
+__device__ __forceinline__ void update_shift(T (&v)[JB], T l, const T* row, int lim)
 {
-    if constexpr(sizeof(T) == 8)
-    {
 #pragma unroll
-        for(int i = 0; i < JB; i += 2)
+    for(int g = 0; g < JB; g += 8)
+    {
+        if(g > lim)
+            break;
+        if constexpr(sizeof(T) == 8)
         {
-            const double2 t = *reinterpret_cast<const double2*>(row + i);
-            if(i + 1 < JB)
-                v[i] = fma(-l, t.x, v[i + 1]);
-            if(i + 2 < JB)
-                v[i + 1] = fma(-l, t.y, v[i + 2]);
+#pragma unroll
+            for(int i = g; i < g + 8 && i < JB; i += 2)
+            {
+                const double2 t = *reinterpret_cast<const double2*>(row + i);
+                if(i + 1 < JB)
+                    v[i] = fma(-l, t.x, v[i + 1]);
+                if(i + 2 < JB)
+                    v[i + 1] = fma(-l, t.y, v[i + 2]);
+            }
         }
-    }
-    else
-    {
-#pragma unroll
-        for(int i = 0; i < JB; i += 4)
+        else
         {
-            const float4 t = *reinterpret_cast<const float4*>(row + i);
-            const float e[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
-            for(int u = 0; u < 4; ++u)
-                if(i + u + 1 < JB)
-                    v[i + u] = fmaf(-l, e[u], v[i + u + 1]);
+            for(int i = g; i < g + 8 && i < JB; i += 4)
+            {
+                const float4 t = *reinterpret_cast<const float4*>(row + i);
+                const float e[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                for(int u = 0; u < 4; ++u)
+                    if(i + u + 1 < JB)
+                        v[i + u] = fmaf(-l, e[u], v[i + u + 1]);
+            }
         }
     }
 }
@@ -423,7 +432,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                         const T x = pv[q][0];
                         const T l = mode == 1 ? x * rcp : (mode == 2 ? x / pivv : x);
                         sP[c * ldp + slot] = -l;
-                        update_shift<T, JB>(pv[q], l, prowv);
+                        update_shift<T, JB>(pv[q], l, prowv, jb - c - 2);
                     }
                 }
             }
