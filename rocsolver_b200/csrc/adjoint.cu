@@ -15,7 +15,7 @@
 namespace rsb {
 
 template <typename T, int NT, int NRC>
-__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 1)
+__global__ void __launch_bounds__(NT, 2)
     solve_adjoint_kernel(int kind, int n, int nrhs, Batch<T> A, int lda, const int* ipiv,
                          int64_t strideP, Batch<T> X, int ldx, Batch<T> G, int ldg, Batch<T> GA,
                          int ldga, Batch<T> GB, int ldgb)
@@ -23,9 +23,10 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 1)
     // kind: 0 = LU (getrf factors), 1 = Cholesky lower, 2 = Cholesky upper
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sdiag = reinterpret_cast<T*>(smem_raw); // staged diagonal blocks
-    T* sg = sdiag + SDIAG_ELEMS;               // n x NRC  (gB columns of the group)
+    T* sg = sdiag + sweep_scratch<NT>();       // n x NRC  (gB columns of the group)
     T* sx = sg + (size_t)n * NRC;              // n x NRC  (X columns of the group)
     int* perm = reinterpret_cast<int*>(sx + (size_t)n * NRC);
+    int* pinv = perm + n; // pinv[perm[i]] = i
     const int64_t b = blockIdx.x;
     const T* a = A.at(b);
     const T* x = X.at(b);
@@ -33,7 +34,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 1)
     T* ga = GA.at(b);
     T* gb = GB.at(b);
     if(kind == 0)
+    {
         build_perm(ipiv + b * strideP, n, perm);
+        for(int i = threadIdx.x; i < n; i += NT)
+            pinv[perm[i]] = i;
+        __syncthreads();
+    }
     for(int c0 = 0; c0 < nrhs; c0 += NRC)
     {
         const int nc = min(NRC, nrhs - c0);
@@ -47,18 +53,18 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 1)
         if(kind == 0)
         {
             // A' y = g  with  A = P' L U  ->  U' L' (P y) = g
-            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
-            block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
+            block_sweep<T, NT, NRC, true>(false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
+            block_sweep<T, NT, NRC, false>(true, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
         }
         else if(kind == 1)
         {
-            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, 1, lda}, n, sg, nc, sdiag);
-            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
+            block_sweep<T, NT, NRC, true>(false, TriView<T>{a, 1, lda}, n, sg, nc, sdiag);
+            block_sweep<T, NT, NRC, false>(false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
         }
         else
         {
-            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
-            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sg, nc, sdiag);
+            block_sweep<T, NT, NRC, true>(false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
+            block_sweep<T, NT, NRC, false>(false, TriView<T>{a, 1, lda}, n, sg, nc, sdiag);
         }
         // gB (inverse row interchanges for LU: gB[perm[i]] = y[i])
         for(int e = threadIdx.x; e < n * nc; e += NT)
@@ -67,12 +73,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 1)
             const int dst = kind == 0 ? perm[i] : i;
             gb[ix(dst, c0 + c, ldgb)] = sg[i + c * n];
         }
-        // gA -= gB X' over this group: row i of gB is sg[perm^{-1}...]; address gB by its
-        // final row: for LU, final row perm[i] holds sg[i]
+        // gA -= gB X' over this group, threads along gA's rows (coalesced stores): row r of
+        // gB is sg[pinv[r]] for LU (final row perm[i] holds sg[i]), sg[r] otherwise
         for(int e = threadIdx.x; e < n * n; e += NT)
         {
-            const int i = e % n, j = e / n; // gA(r, j) with r = final row of sg[i]
-            const int r = kind == 0 ? perm[i] : i;
+            const int r = e % n, j = e / n;
+            const int i = kind == 0 ? pinv[r] : r;
             T acc = c0 == 0 ? T(0) : ga[ix(r, j, ldga)];
 #pragma unroll
             for(int c = 0; c < NRC; ++c)
@@ -91,7 +97,8 @@ rocblas_status launch_solve_adjoint(cudaStream_t s, int kind, int n, int nrhs, B
 {
     constexpr int NT = 256;
     constexpr int NRC = 8;
-    const size_t smem = sizeof(T) * (2 * (size_t)n * NRC + SDIAG_ELEMS) + sizeof(int) * (size_t)n;
+    const size_t smem =
+        sizeof(T) * (2 * (size_t)n * NRC + sweep_scratch<NT>()) + sizeof(int) * 2 * (size_t)n;
     if(smem > 200 * 1024)
         return rocblas_status_not_implemented;
     auto k = solve_adjoint_kernel<T, NT, NRC>;

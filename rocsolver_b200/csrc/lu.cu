@@ -207,7 +207,8 @@ static rocblas_status run_getrs_cta_nt(cudaStream_t s, int trans, int n, int nrh
                                        int lda, const int* ipiv, int64_t sP, Batch<T> B,
                                        int ldb, const int* skip, int bc, Gate g)
 {
-    const size_t smem = sizeof(T) * ((size_t)n * NRC + SDIAG_ELEMS) + sizeof(int) * (size_t)n;
+    const size_t smem =
+        sizeof(T) * ((size_t)n * NRC + sweep_scratch<NT>()) + sizeof(int) * (size_t)n;
     auto k = getrs_cta_kernel<T, NT, NRC>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
@@ -333,7 +334,7 @@ template <typename T, int NT, int NRC>
 static rocblas_status run_potrs_nt(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A,
                                    int lda, Batch<T> B, int ldb, const int* skip, int bc)
 {
-    const size_t smem = sizeof(T) * ((size_t)n * NRC + SDIAG_ELEMS);
+    const size_t smem = sizeof(T) * ((size_t)n * NRC + sweep_scratch<NT>());
     auto k = potrs_cta_kernel<T, NT, NRC>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;

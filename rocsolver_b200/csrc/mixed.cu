@@ -476,10 +476,10 @@ __global__ void __launch_bounds__(NT, REFINE_CTAS_PER_SM)
     double* rs = xs + (size_t)n * nrhs;                    // n x nrhs
     double* red = rs + (size_t)n * nrhs;                   // NT/32
     float* sdiag = reinterpret_cast<float*>(red + NT / 32); // staged diagonal blocks
-    float* s32 = sdiag + SDIAG_ELEMS;                       // n x NRC
+    const bool blockinv = n <= REFINE_BLOCKINV_MAXN;
+    float* s32 = sdiag + (blockinv ? SDIAG_ELEMS : sweep_scratch<NT>()); // n x NRC
     int* perm = reinterpret_cast<int*>(s32 + (size_t)n * NRC);
     float* sinv = reinterpret_cast<float*>(perm + ((n + 3) & ~3)); // [2*nblk][32x33]
-    const bool blockinv = n <= REFINE_BLOCKINV_MAXN;
     double* part = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(sinv + (blockinv ? 2 * ((n + 31) / 32) * BI_ELEMS : 0))
          + 15)
@@ -544,9 +544,9 @@ __global__ void __launch_bounds__(NT, REFINE_CTAS_PER_SM)
             }
             else
             {
-                block_sweep<float, NT, NRC>(true, true, TriView<float>{lu, 1, n}, n, s32, nc,
+                block_sweep<float, NT, NRC, true>(true, TriView<float>{lu, 1, n}, n, s32, nc,
                                             sdiag);
-                block_sweep<float, NT, NRC>(false, false, TriView<float>{lu, 1, n}, n, s32, nc,
+                block_sweep<float, NT, NRC, false>(false, TriView<float>{lu, 1, n}, n, s32, nc,
                                             sdiag);
             }
             for(int e = tid; e < n * nc; e += NT)
@@ -649,7 +649,8 @@ static size_t refine_smem(int n, int nrhs, int NRC, int NT)
     const size_t inv = n <= REFINE_BLOCKINV_MAXN ? 2 * nblk * BI_ELEMS : 0;
     const size_t part = 2 * n <= NT ? (size_t)(NRC + 1) * n : 0;
     return sizeof(double) * (2 * (size_t)n * nrhs + NT / 32)
-           + sizeof(float) * ((size_t)n * NRC + SDIAG_ELEMS + inv)
+           + sizeof(float) * ((size_t)n * NRC + (inv ? SDIAG_ELEMS : (size_t)sweep_scratch<REFINE_NT>())
+                              + inv)
            + sizeof(int) * (size_t)((n + 3) & ~3) + sizeof(double) * part + 16;
 }
 

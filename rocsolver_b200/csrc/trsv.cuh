@@ -32,122 +32,193 @@ struct TriView
 constexpr int SDIAG_LD = 33;               // staged diagonal block, padded
 constexpr int SDIAG_ELEMS = 32 * SDIAG_LD;
 
-// Solve M x = b in place for the nc columns of sb (ld = n).  forward: M lower
-// (substitution top-down), else M upper (bottom-up).  unit: unit diagonal.
-// sdiag: shared scratch of SDIAG_ELEMS elements.  Must be called by all NT threads.
-// Per 32-wide block: all threads stage the diagonal block in shared memory (coalesced
-// along the operand's contiguous direction), warp 0 solves it with shuffles, then all
-// threads apply it to the remaining rows with independent (unrolled) factor loads.
-template <typename T, int NT, int NRC>
-__device__ void block_sweep(bool forward, bool unit, TriView<T> M, int n, T* sb, int nc,
-                            T* sdiag)
+// Scratch (elements) block_sweep needs: one inverted 32x32 diagonal block per warp, and
+// the solved block's values for up to 32 right-hand sides.
+template <int NT>
+__host__ __device__ constexpr int sweep_scratch()
 {
-    const unsigned full = 0xffffffffu;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nblk = (n + 31) / 32;
-    for(int bi = 0; bi < nblk; ++bi)
+    return (NT / 32) * SDIAG_ELEMS + 32 * 32;
+}
+
+// Invert the diagonal block M(kb.., kb..) (order nb <= 32, padded with the identity) with
+// one warp, in place in blk (row-major, blk[i*SDIAG_LD + k]): the block is staged
+// coalesced along M's contiguous direction, then lane j computes column j of the inverse
+// eight rows at a time (LOWER: top-down, else bottom-up): the rows already finished
+// contribute through shared memory, the eight new rows are solved in registers, written
+// over the block's rows once every lane has read them, and the next eight follow.  Few
+// registers, so the sweep kernels keep their occupancy.  unit: unit diagonal.
+template <typename T, bool LOWER>
+__device__ __forceinline__ void invert_block(bool unit, TriView<T> M, int kb, int nb, T* blk)
+{
+    const int lane = threadIdx.x & 31;
+    for(int e = lane; e < 32 * 32; e += 32)
     {
-        const int kb = forward ? bi * 32 : (nblk - 1 - bi) * 32;
-        const int nb = min(32, n - kb);
-        for(int e = tid; e < nb * nb; e += NT)
+        int i, k; // M's contiguous direction first
+        if(M.rs == 1)
         {
-            int r, c;
-            if(M.rs == 1)
+            i = e & 31;
+            k = e >> 5;
+        }
+        else
+        {
+            k = e & 31;
+            i = e >> 5;
+        }
+        T v;
+        if(i >= nb || k >= nb)
+            v = i == k ? T(1) : T(0);
+        else if(i == k)
+            v = unit ? T(1) : M(kb + i, kb + k);
+        else
+            v = (LOWER ? i > k : i < k) ? M(kb + i, kb + k) : T(0);
+        blk[i * SDIAG_LD + k] = v;
+    }
+    __syncwarp();
+#pragma unroll 1
+    for(int rb = 0; rb < 4; ++rb)
+    {
+        const int r0 = LOWER ? 8 * rb : 24 - 8 * rb; // first row of this group
+        T x[8];
+#pragma unroll
+        for(int u = 0; u < 8; ++u)
+            x[u] = r0 + u == lane ? T(1) : T(0);
+        // finished rows: above the group (LOWER) or below it
+        const int k0 = LOWER ? 0 : r0 + 8, k1 = LOWER ? r0 : 32;
+#pragma unroll 4
+        for(int k = k0; k < k1; ++k)
+        {
+            const T xk = blk[k * SDIAG_LD + lane];
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
+                x[u] = fma(-blk[(r0 + u) * SDIAG_LD + k], xk, x[u]);
+        }
+        // the group's own rows
+        if constexpr(LOWER)
+        {
+#pragma unroll
+            for(int u = 0; u < 8; ++u)
             {
-                r = e % nb;
-                c = e / nb;
+#pragma unroll
+                for(int v = 0; v < u; ++v)
+                    x[u] = fma(-blk[(r0 + u) * SDIAG_LD + r0 + v], x[v], x[u]);
+                if(!unit)
+                    x[u] = x[u] / blk[(r0 + u) * SDIAG_LD + r0 + u];
             }
-            else
+        }
+        else
+        {
+#pragma unroll
+            for(int u = 7; u >= 0; --u)
             {
-                c = e % nb;
-                r = e / nb;
+#pragma unroll
+                for(int v = u + 1; v < 8; ++v)
+                    x[u] = fma(-blk[(r0 + u) * SDIAG_LD + r0 + v], x[v], x[u]);
+                if(!unit)
+                    x[u] = x[u] / blk[(r0 + u) * SDIAG_LD + r0 + u];
             }
-            sdiag[c * SDIAG_LD + r] = M(kb + r, kb + c);
+        }
+        __syncwarp();
+#pragma unroll
+        for(int u = 0; u < 8; ++u)
+            blk[(r0 + u) * SDIAG_LD + lane] = x[u];
+        __syncwarp();
+    }
+}
+
+// Solve M x = b in place for the nc columns of sb (ld = n).  FORWARD: M lower
+// (substitution top-down), else M upper (bottom-up).  unit: unit diagonal.
+// sinv: shared scratch of sweep_scratch<NT>() elements.  Must be called by all NT threads.
+// The 32-wide diagonal blocks are taken in chunks of NT/32: every warp inverts one block
+// of the chunk in parallel (off the sweep's serial path), then per block the threads
+// apply the inverse (a 32x32 product, no serial chain) and all threads apply the block's
+// columns to the remaining rows with independent (unrolled) factor loads.  The block
+// product is spread over all threads (one row and right-hand side each).  Explicit
+// inverses of the diagonal blocks are also what the reference's batched trsm uses
+// (rocBLAS trsm with invA).
+template <typename T, int NT, int NRC, bool FORWARD>
+__device__ void block_sweep(bool unit, TriView<T> M, int n, T* sb, int nc, T* sinv)
+{
+    constexpr bool forward = FORWARD;
+    constexpr int NW = NT / 32;
+    static_assert(NRC <= 32, "right-hand sides per pass");
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int nblk = (n + 31) / 32;
+    T* sy = sinv + NW * SDIAG_ELEMS; // [NRC][32]
+    for(int cb = 0; cb < nblk; cb += NW)
+    {
+        {
+            const int bi = cb + warp;
+            if(bi < nblk)
+            {
+                const int kb = forward ? bi * 32 : (nblk - 1 - bi) * 32;
+                invert_block<T, FORWARD>(unit, M, kb, min(32, n - kb), sinv + warp * SDIAG_ELEMS);
+            }
         }
         __syncthreads();
-        if(warp == 0)
+        const int cend = min(cb + NW, nblk);
+        for(int bi = cb; bi < cend; ++bi)
         {
-            T x[NRC];
-#pragma unroll
-            for(int c = 0; c < NRC; ++c)
-                x[c] = (lane < nb && c < nc) ? sb[kb + lane + c * n] : T(0);
-            if(forward)
+            const int kb = forward ? bi * 32 : (nblk - 1 - bi) * 32;
+            const int nb = min(32, n - kb);
+            const T* inv = sinv + (bi - cb) * SDIAG_ELEMS;
+            // y = inv * b_block for every right-hand side: one output (row, rhs) per thread,
+            // written to the side buffer sy so that no thread overwrites an input
+            for(int o = tid; o < 32 * nc; o += NT)
             {
-                for(int k = 0; k < nb; ++k)
+                const int row = o & 31, c = o >> 5;
+                T y0 = T(0), y1 = T(0);
+#pragma unroll 4
+                for(int j = 0; j < 32; j += 2)
                 {
-                    const T mlk = sdiag[k * SDIAG_LD + lane];
-                    const T dkk = unit ? T(1) : sdiag[k * SDIAG_LD + k];
+                    if(j < nb)
+                        y0 = fma(inv[row * SDIAG_LD + j], sb[kb + j + c * n], y0);
+                    if(j + 1 < nb)
+                        y1 = fma(inv[row * SDIAG_LD + j + 1], sb[kb + j + 1 + c * n], y1);
+                }
+                sy[row + 32 * c] = y0 + y1;
+            }
+            __syncthreads();
+            for(int o = tid; o < 32 * nc; o += NT)
+                if((o & 31) < nb)
+                    sb[kb + (o & 31) + (o >> 5) * n] = sy[o];
+            // rows outside the block: forward -> below it, backward -> above it
+            const int r0 = forward ? kb + nb : 0;
+            const int r1 = forward ? n : kb;
+            for(int i = r0 + tid; i < r1; i += NT)
+            {
+                T acc[NRC];
 #pragma unroll
-                    for(int c = 0; c < NRC; ++c)
+                for(int c = 0; c < NRC; ++c)
+                    acc[c] = c < nc ? sb[i + c * n] : T(0);
+                if(nb == 32)
+                {
+                    T mv[32];
+#pragma unroll
+                    for(int k = 0; k < 32; ++k)
+                        mv[k] = M(i, kb + k);
+#pragma unroll
+                    for(int k = 0; k < 32; ++k)
+#pragma unroll
+                        for(int c = 0; c < NRC; ++c)
+                            acc[c] = fma(-mv[k], sy[k + 32 * c], acc[c]);
+                }
+                else
+                {
+                    for(int k = 0; k < nb; ++k)
                     {
-                        if(!unit && lane == k)
-                            x[c] = x[c] / dkk;
-                        const T xk = __shfl_sync(full, x[c], k);
-                        if(lane > k && lane < nb)
-                            x[c] = fma(-mlk, xk, x[c]);
+                        const T mik = M(i, kb + k);
+#pragma unroll
+                        for(int c = 0; c < NRC; ++c)
+                            acc[c] = fma(-mik, sy[k + 32 * c], acc[c]);
                     }
                 }
-            }
-            else
-            {
-                for(int k = nb - 1; k >= 0; --k)
-                {
-                    const T mlk = sdiag[k * SDIAG_LD + lane];
-                    const T dkk = unit ? T(1) : sdiag[k * SDIAG_LD + k];
 #pragma unroll
-                    for(int c = 0; c < NRC; ++c)
-                    {
-                        if(!unit && lane == k)
-                            x[c] = x[c] / dkk;
-                        const T xk = __shfl_sync(full, x[c], k);
-                        if(lane < k)
-                            x[c] = fma(-mlk, xk, x[c]);
-                    }
-                }
+                for(int c = 0; c < NRC; ++c)
+                    if(c < nc)
+                        sb[i + c * n] = acc[c];
             }
-#pragma unroll
-            for(int c = 0; c < NRC; ++c)
-                if(lane < nb && c < nc)
-                    sb[kb + lane + c * n] = x[c];
+            __syncthreads();
         }
-        __syncthreads();
-        // rows outside the block: forward -> below it, backward -> above it
-        const int r0 = forward ? kb + nb : 0;
-        const int r1 = forward ? n : kb;
-        for(int i = r0 + tid; i < r1; i += NT)
-        {
-            T acc[NRC];
-#pragma unroll
-            for(int c = 0; c < NRC; ++c)
-                acc[c] = c < nc ? sb[i + c * n] : T(0);
-            if(nb == 32)
-            {
-                T mv[32];
-#pragma unroll
-                for(int k = 0; k < 32; ++k)
-                    mv[k] = M(i, kb + k);
-#pragma unroll
-                for(int k = 0; k < 32; ++k)
-#pragma unroll
-                    for(int c = 0; c < NRC; ++c)
-                        acc[c] = fma(-mv[k], sb[kb + k + c * n], acc[c]);
-            }
-            else
-            {
-                for(int k = 0; k < nb; ++k)
-                {
-                    const T mik = M(i, kb + k);
-#pragma unroll
-                    for(int c = 0; c < NRC; ++c)
-                        acc[c] = fma(-mik, sb[kb + k + c * n], acc[c]);
-                }
-            }
-#pragma unroll
-            for(int c = 0; c < NRC; ++c)
-                if(c < nc)
-                    sb[i + c * n] = acc[c];
-        }
-        __syncthreads();
     }
 }
 
@@ -240,13 +311,13 @@ __device__ __forceinline__ void getrs_dev(int trans, int n, int nrhs, const T* a
         __syncthreads();
         if(!trans)
         {
-            block_sweep<T, NT, NRC>(true, true, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
-            block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
+            block_sweep<T, NT, NRC, true>(true, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
+            block_sweep<T, NT, NRC, false>(false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
         }
         else
         {
-            block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
-            block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
+            block_sweep<T, NT, NRC, true>(false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
+            block_sweep<T, NT, NRC, false>(true, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
         }
         for(int e = threadIdx.x; e < n * nc; e += NT)
         {
@@ -268,7 +339,7 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sdiag = reinterpret_cast<T*>(smem_raw);
-    T* sb = sdiag + SDIAG_ELEMS;
+    T* sb = sdiag + sweep_scratch<NT>();
     int* perm = reinterpret_cast<int*>(sb + (size_t)n * NRC);
     const int groups = (nrhs + NRC - 1) / NRC;
     const int64_t b = blockIdx.x / groups;
@@ -290,13 +361,13 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
     __syncthreads();
     if(!trans)
     {
-        block_sweep<T, NT, NRC>(true, true, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
-        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC, true>(true, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC, false>(false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
     }
     else
     {
-        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
-        block_sweep<T, NT, NRC>(false, true, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC, true>(false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC, false>(true, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
     }
     for(int e = threadIdx.x; e < n * nc; e += NT)
     {
@@ -315,7 +386,7 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sdiag = reinterpret_cast<T*>(smem_raw);
-    T* sb = sdiag + SDIAG_ELEMS;
+    T* sb = sdiag + sweep_scratch<NT>();
     const int groups = (nrhs + NRC - 1) / NRC;
     const int64_t b = blockIdx.x / groups;
     const int c0 = (blockIdx.x % groups) * NRC;
@@ -332,13 +403,13 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
     __syncthreads();
     if(!upper)
     {
-        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
-        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC, true>(false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC, false>(false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
     }
     else
     {
-        block_sweep<T, NT, NRC>(true, false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
-        block_sweep<T, NT, NRC>(false, false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC, true>(false, TriView<T>{a, lda, 1}, n, sb, nc, sdiag);
+        block_sweep<T, NT, NRC, false>(false, TriView<T>{a, 1, lda}, n, sb, nc, sdiag);
     }
     for(int e = threadIdx.x; e < n * nc; e += NT)
     {

@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(NT, 2)
         if(v.mode != 1 && (v.mode == 2 || v.info[b] == 0))
         {
             T* sdiag = reinterpret_cast<T*>(smem_raw);
-            T* sb = sdiag + SDIAG_ELEMS;
+            T* sb = sdiag + sweep_scratch<NT>();
             int* perm = reinterpret_cast<int*>(sb + (size_t)v.max_n * 4);
             getrs_dev<T, NT, 4>(0, n, v.nrhs[b], A[b], v.lda[b], v.ipiv[b], B[b], v.ldb[b], sb,
                                 perm, sdiag);
@@ -253,7 +253,7 @@ static rocblas_status run_vb(cudaStream_t s, VbArgs v, T* const* A, T* const* B,
         if(s1 > smem)
             smem = s1;
     }
-    const size_t solve = sizeof(T) * ((size_t)v.max_n * 4 + SDIAG_ELEMS)
+    const size_t solve = sizeof(T) * ((size_t)v.max_n * 4 + sweep_scratch<NT>())
                          + sizeof(int) * (size_t)v.max_n;
     if(solve > smem)
         smem = solve;
