@@ -66,24 +66,41 @@ __global__ void __launch_bounds__(NT, 2)
             block_sweep<T, NT, NRC, true>(false, TriView<T>{a, lda, 1}, n, sg, nc, sdiag);
             block_sweep<T, NT, NRC, false>(false, TriView<T>{a, 1, lda}, n, sg, nc, sdiag);
         }
-        // gB (inverse row interchanges for LU: gB[perm[i]] = y[i])
+        // gB (inverse row interchanges for LU: gB[perm[i]] = y[i], i.e. row r of gB is
+        // y[pinv[r]]), stored along gB's rows
         for(int e = threadIdx.x; e < n * nc; e += NT)
         {
-            const int i = e % n, c = e / n;
-            const int dst = kind == 0 ? perm[i] : i;
-            gb[ix(dst, c0 + c, ldgb)] = sg[i + c * n];
+            const int r = e % n, c = e / n;
+            const int src = kind == 0 ? pinv[r] : r;
+            gb[ix(r, c0 + c, ldgb)] = sg[src + c * n];
         }
-        // gA -= gB X' over this group, threads along gA's rows (coalesced stores): row r of
-        // gB is sg[pinv[r]] for LU (final row perm[i] holds sg[i]), sg[r] otherwise
-        for(int e = threadIdx.x; e < n * n; e += NT)
+        // gA -= gB X' over this group: each thread keeps one row r of gB (its NRC values,
+        // sg[pinv[r]] for LU since final row perm[i] holds sg[i]) in registers and walks
+        // columns j; consecutive threads take consecutive rows (coalesced stores), and
+        // when n <= NT the NT/n thread groups split the columns
         {
-            const int r = e % n, j = e / n;
-            const int i = kind == 0 ? pinv[r] : r;
-            T acc = c0 == 0 ? T(0) : ga[ix(r, j, ldga)];
+            const int P = n <= NT ? NT / n : 1;
+            const int g = n <= NT ? (int)threadIdx.x / n : 0;
+            const int rstep = n <= NT ? n : NT;
+            for(int r = n <= NT ? (int)threadIdx.x % n : (int)threadIdx.x; r < n && g < P;
+                r += rstep)
+            {
+                const int i = kind == 0 ? pinv[r] : r;
+                T gr[NRC];
 #pragma unroll
-            for(int c = 0; c < NRC; ++c)
-                acc = fma(-sg[i + c * n], sx[j + c * n], acc);
-            ga[ix(r, j, ldga)] = acc;
+                for(int c = 0; c < NRC; ++c)
+                    gr[c] = c < nc ? sg[i + c * n] : T(0);
+                for(int j = g; j < n; j += P)
+                {
+                    T acc = c0 == 0 ? T(0) : ga[ix(r, j, ldga)];
+#pragma unroll
+                    for(int c = 0; c < NRC; ++c)
+                        acc = fma(-gr[c], sx[j + c * n], acc);
+                    ga[ix(r, j, ldga)] = acc;
+                }
+                if(n <= NT)
+                    break;
+            }
         }
         __syncthreads();
     }
