@@ -18,6 +18,12 @@ configurations; no dataset is involved):
               (plain FP64).  Metric: solves/s.
   getrf_n32   n=32, lda 32, batch 1000, nrhs 1, U[-1,1] from seed 0: dgetrf + dgetrs.
   potrf_n64   n=64, batch 20000, nrhs 4, A = G G' + n I: dpotrf + dpotrs.
+  vbatched_4096  4096 members, n ~ U[8, 512], nrhs ~ U[1, 16], A ~ U[-1,1] + 0.1 n I:
+              rocsolver_dgesv_vbatched captured once in a CUDA graph and replayed; reported
+              next to the same members solved by per-size launches (dgetrf_batched +
+              dgetrs_batched per distinct n, "per_size_launches").
+  adjoint_n128   n=128, batch 8192, nrhs 8, FP64, A ~ U[-1,1] + 4 I factored once outside
+              the timing, G ~ N(0,1): rocsolver_dgetrs_adjoint_strided_batched (gB, gA).
 Inputs are larger than L2 (126 MB) for gesv_n256 and potrf_n64; getrf_n32 (8 MB) rotates
 through 24 distinct copies of the batch so each step reads cold data.
 
@@ -46,7 +52,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="dsgesv_n256",
-                   choices=["dsgesv_n256", "gesv_n256", "getrf_n32", "potrf_n64"])
+                   choices=["dsgesv_n256", "gesv_n256", "getrf_n32", "potrf_n64",
+                            "vbatched_4096", "adjoint_n128"])
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target CPU time of the bounded CPU-baseline sample")
     return p.parse_args()
@@ -495,6 +502,8 @@ def main():
 
     if args.impl == "reference":
         return main_reference(args, rank, world)
+    if args.workload in ("vbatched_4096", "adjoint_n128"):
+        return main_extra(args, rank, world, local)
 
     import torch
     import rocsolver_b200 as rs
@@ -589,10 +598,14 @@ def main_reference(args, rank, world):
         return
     import torch
     dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
-    w = build_workload(args.workload, torch, None, dev, None)
+    extra = args.workload in ("vbatched_4096", "adjoint_n128")
+    w = (_extra_workload(args.workload, torch, dev) if extra
+         else build_workload(args.workload, torch, None, dev, None))
+    w.dtype = getattr(w, "dtype", "f64")
     vals = []
     for i in range(args.warmup + args.steps):
-        r = cpu_sample(w, max(1.0, args.cpu_seconds / max(1, args.steps)))
+        sample = cpu_sample_extra if extra else cpu_sample
+        r = sample(w, max(1.0, args.cpu_seconds / max(1, args.steps)))
         if i >= args.warmup:
             vals.append(r["value"])
     v = statistics.median(vals)
@@ -604,6 +617,352 @@ def main_reference(args, rank, world):
                              "sample": r["sample"]},
             "e2e": {"value": v, "unit": w.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- extra rows
+def _vb_inputs(torch, dev, bc, nmax, seed):
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    sizes = torch.randint(8, nmax + 1, (bc,), generator=g, device=dev, dtype=torch.int32)
+    rhs = torch.randint(1, 17, (bc,), generator=g, device=dev, dtype=torch.int32)
+    A = torch.rand(bc, nmax, nmax, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    A += 0.1 * sizes.double()[:, None, None] * torch.eye(nmax, device=dev, dtype=torch.float64)
+    B = torch.rand(bc, 16, nmax, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    # member b: n_b x n_b column-major in an nmax x nmax slot (lda = nmax); B: nmax x 16
+    return sizes, rhs, A.transpose(1, 2).contiguous(), B.contiguous()
+
+
+def _extra_workload(name, torch, dev):
+    w = Workload()
+    w.name = name
+    if name == "vbatched_4096":
+        w.bc, w.nmax = 4096, 512
+        w.sizes, w.rhs, w.A0, w.B0 = _vb_inputs(torch, dev, w.bc, w.nmax, 11)
+        w.metric = "variable-size batched solves/s (FP64 gesv_vbatched, n~U[8,512], nrhs~U[1,16])"
+        w.unit = "solves/s"
+        w.config = {"workload": "rocsolver_dgesv_vbatched, 4096 members, n ~ U[8,512], "
+                                "nrhs ~ U[1,16], A ~ U[-1,1] + 0.1 n I, one persistent launch "
+                                "(plus the plan kernel) replayed from a CUDA graph",
+                    "batch": w.bc, "n_max": w.nmax,
+                    "l2": "inputs 8.6 GB > L2; A and B restored between steps outside the "
+                          "timed events"}
+        n = w.sizes.double()
+        k = w.rhs.double()
+        w.bytes_total = float((2 * n * n * 8 + 2 * n * k * 8 + 4 * n + 4).sum())
+        w.flops_total = float((2 * n ** 3 / 3 + 2 * n * n * k).sum())
+    else:
+        w.bc, w.n, w.nrhs = 8192, 128, 8
+        g = torch.Generator(device=dev)
+        g.manual_seed(12)
+        n, bc, nrhs = w.n, w.bc, w.nrhs
+        A = torch.rand(bc, n, n, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+        A += 4 * torch.eye(n, device=dev, dtype=torch.float64)
+        w.Arow = A
+        w.A0 = A.transpose(1, 2).contiguous()
+        w.X0 = torch.randn(bc, nrhs, n, generator=g, device=dev, dtype=torch.float64)
+        w.G0 = torch.randn(bc, nrhs, n, generator=g, device=dev, dtype=torch.float64)
+        w.metric = "batched solve adjoints/s (FP64 getrs_adjoint: gB = A^-T G, gA = -gB X')"
+        w.unit = "adjoints/s"
+        w.config = {"workload": "rocsolver_dgetrs_adjoint_strided_batched, n=128, batch 8192, "
+                                "nrhs 8, A ~ U[-1,1] + 4 I factored once (not timed), "
+                                "G ~ N(0,1)", "n": n, "batch": bc, "nrhs": nrhs,
+                    "l2": "factors 1 GiB > L2"}
+        w.bytes_total = bc * (2 * n * n * 8 + 4 * n * nrhs * 8 + 4 * n)
+        w.flops_total = bc * (4.0 * n * n * nrhs)
+    return w
+
+
+def main_extra(args, rank, world, local):
+    """The variable-size and adjoint rows: same contract as main() (one JSON line on rank
+    0, device time = max over ranks, e2e through the C ABI with host buffers)."""
+    import torch
+    import rocsolver_b200 as rs
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    handle = rs.Handle(torch.cuda.current_stream().cuda_stream)
+    h = handle.value
+    extra_handles = []
+    graph = None
+    w = _extra_workload(args.workload, torch, dev)
+    stream = torch.cuda.current_stream()
+    P = rs.ptr
+    bc = w.bc
+    extra = {}
+    if w.name == "vbatched_4096":
+        nmax = w.nmax
+        A, B = w.A0.clone(), w.B0.clone()
+        ld = torch.full((bc,), nmax, dtype=torch.int32, device=dev)
+        ipiv = torch.zeros(bc * nmax, dtype=torch.int32, device=dev)
+        info = torch.zeros(bc, dtype=torch.int32, device=dev)
+        ar = torch.arange(bc, device=dev, dtype=torch.int64)
+        pa = ar * (nmax * nmax * 8) + A.data_ptr()
+        pb = ar * (16 * nmax * 8) + B.data_ptr()
+        pp = ar * (nmax * 4) + ipiv.data_ptr()
+
+        # captured on a side stream with its own handle (a graph cannot capture the legacy
+        # default stream); replays run on the current stream
+        cap = torch.cuda.Stream()
+        hcap = rs.Handle(cap.cuda_stream)
+        extra_handles = [hcap]
+
+        def call():
+            rs.check(rs.call("rocsolver_dgesv_vbatched", hcap.value, P(w.sizes), P(w.rhs), P(pa),
+                             P(ld), P(pp), P(pb), P(ld), P(info), nmax, 16, bc), "gesv_vbatched")
+
+        def restore():
+            A.copy_(w.A0)
+            B.copy_(w.B0)
+
+        restore()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(cap):
+            call()  # sizes the workspace before capture
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=cap):
+            call()
+        torch.cuda.synchronize()
+        run = graph.replay
+        launches = 2
+    else:
+        n, nrhs = w.n, w.nrhs
+        LU = w.A0.clone()
+        ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
+        info = torch.zeros(bc, dtype=torch.int32, device=dev)
+        rs.check(rs.call("rocsolver_dgetrf_strided_batched", h, n, n, P(LU), n, n * n, P(ipiv),
+                         n, P(info), bc), "getrf")
+        gA = torch.empty_like(LU)
+        gB = torch.empty_like(w.G0)
+
+        def call():
+            rs.check(rs.call("rocsolver_dgetrs_adjoint_strided_batched", h, n, nrhs, P(LU), n,
+                             n * n, P(ipiv), n, P(w.X0), n, n * nrhs, P(w.G0), n, n * nrhs,
+                             P(gA), n, n * n, P(gB), n, n * nrhs, bc), "adjoint")
+
+        def restore():
+            pass
+
+        run = call
+        launches = 1
+    for _ in range(args.warmup):
+        restore()
+        run()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    time.sleep(0.3)
+    for i in range(args.steps):
+        restore()
+        ev[i][0].record(stream)
+        run()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in ev)
+    if pg:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / args.steps
+    peaks = load_peaks()
+    gbs = w.bytes_total / (ms / 1e3) / 1e9
+    # accuracy and the comparison arm
+    if w.name == "vbatched_4096":
+        restore()
+        run()
+        torch.cuda.synchronize()
+        sz, kk = w.sizes.cpu().numpy(), w.rhs.cpu().numpy()
+        A0, B0, X = w.A0.cpu().numpy(), w.B0.cpu().numpy(), B.cpu().numpy()
+        worst = 0.0
+        for b in range(0, bc, 16):  # every 16th member, host check
+            nb, kb = int(sz[b]), int(kk[b])
+            Ab = A0[b][:nb, :nb].T  # A0[b][j][i] holds a_ij (column-major, lda = nmax)
+            xb = X[b][:kb, :nb].T
+            bb = B0[b][:kb, :nb].T
+            r = np.abs(Ab @ xb - bb).max() / (np.abs(Ab).sum(1).max() * np.abs(xb).max()
+                                               + np.abs(bb).max())
+            worst = max(worst, r)
+        extra["accuracy"] = {"backward_err_max_sampled": worst,
+                             "info_nonzero": int((info.cpu().numpy() != 0).sum())}
+        # per-size launches: dgetrf_batched + dgetrs_batched per distinct n (nrhs = the
+        # largest nrhs among that size's members; the others solve spare columns)
+        groups = {}
+        for b in range(bc):
+            groups.setdefault(int(sz[b]), []).append(b)
+        plans = []
+        for nb, mem in sorted(groups.items()):
+            idx = torch.tensor(mem, device=dev, dtype=torch.int64)
+            # pointer-array batches take ONE pivot array with stride strideP = n
+            plans.append((nb, int(kk[mem].max()), pa[idx].contiguous(), pb[idx].contiguous(),
+                          torch.zeros(len(mem) * nb, dtype=torch.int32, device=dev), len(mem)))
+
+        def per_size():
+            for nb, kmax, qa, qb, qp, cnt in plans:
+                rs.check(rs.call("rocsolver_dgetrf_batched", h, nb, nb, P(qa), nmax, P(qp), nb,
+                                 P(info), cnt), "getrf_batched")
+                rs.check(rs.call("rocsolver_dgetrs_batched", h, rs.OP_N, nb, kmax, P(qa), nmax,
+                                 P(qp), nb, P(qb), nmax, cnt), "getrs_batched")
+
+        restore()
+        per_size()
+        torch.cuda.synchronize()
+        pev = []
+        for _ in range(3):
+            restore()
+            a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            per_size()
+            b2.record(stream)
+            pev.append((a, b2))
+        torch.cuda.synchronize()
+        pms = statistics.median([a.elapsed_time(b2) for a, b2 in pev])
+        extra["per_size_launches"] = {"value": bc / (pms / 1e3), "unit": w.unit, "ms": pms,
+                                      "launches": 2 * len(plans)}
+        # e2e: A and B from pinned host memory, solutions and info back, every step
+        hA, hB = w.A0.cpu().pin_memory(), w.B0.cpu().pin_memory()
+        hX, hI = torch.empty_like(hB).pin_memory(), torch.empty(bc, dtype=torch.int32).pin_memory()
+
+        def e2e_step():
+            A.copy_(hA, non_blocking=True)
+            B.copy_(hB, non_blocking=True)
+            run()
+            hX.copy_(B, non_blocking=True)
+            hI.copy_(info, non_blocking=True)
+        h2d, d2h = (hA.numel() + hB.numel()) * 8, hX.numel() * 8 + bc * 4
+    else:
+        n, nrhs = w.n, w.nrhs
+        call()
+        torch.cuda.synchronize()
+        # gB against A^{-T} G and gA against -gB X' computed with torch (FP64)
+        Gt = w.G0.transpose(1, 2)
+        gBt = gB.transpose(1, 2)
+        res = torch.bmm(w.Arow.transpose(1, 2), gBt) - Gt
+        rel_b = float((res.abs().amax((1, 2)) / (w.Arow.abs().sum(1).amax(1)
+                                                 * gBt.abs().amax((1, 2)))).max())
+        gA_ref = -torch.bmm(gBt, w.X0)
+        rel_a = float(((gA.transpose(1, 2) - gA_ref).abs().amax((1, 2))
+                       / gA_ref.abs().amax((1, 2))).max())
+        extra["accuracy"] = {"gB_backward_err_max": rel_b, "gA_rel_err_max": rel_a}
+        hLU, hP = LU.cpu().pin_memory(), ipiv.cpu().pin_memory()
+        hX, hG = w.X0.cpu().pin_memory(), w.G0.cpu().pin_memory()
+        hgA, hgB = torch.empty_like(hLU).pin_memory(), torch.empty_like(hG).pin_memory()
+        dLU, dP = torch.empty_like(LU), torch.empty_like(ipiv)
+        dX, dG = torch.empty_like(w.X0), torch.empty_like(w.G0)
+
+        def e2e_step():
+            dLU.copy_(hLU, non_blocking=True)
+            dP.copy_(hP, non_blocking=True)
+            dX.copy_(hX, non_blocking=True)
+            dG.copy_(hG, non_blocking=True)
+            rs.check(rs.call("rocsolver_dgetrs_adjoint_strided_batched", h, n, nrhs, P(dLU), n,
+                             n * n, P(dP), n, P(dX), n, n * nrhs, P(dG), n, n * nrhs, P(gA), n,
+                             n * n, P(gB), n, n * nrhs, bc), "adjoint")
+            hgA.copy_(gA, non_blocking=True)
+            hgB.copy_(gB, non_blocking=True)
+        h2d = (hLU.numel() + hX.numel() + hG.numel()) * 8 + hP.numel() * 4
+        d2h = (hgA.numel() + hgB.numel()) * 8
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k = max(3, min(args.steps, 5))
+    a.record(stream)
+    for _ in range(k):
+        e2e_step()
+    b2.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b2) / k
+    if pg:
+        t = torch.tensor([e2e_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    line = {"metric": w.metric, "value": bc * world / (ms / 1e3), "unit": w.unit,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded, generated on device)", "config": w.config,
+            "gpu_launches": launches * args.steps,
+            "e2e": {"value": bc * world / (e2e_ms / 1e3), "unit": w.unit,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": "vb_persistent_kernel<double>"
+                         if w.name == "vbatched_4096" else "solve_adjoint_kernel<double>",
+                         "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": gbs / peaks["hbm_gbs"], "traffic": None,
+                         "peak_source": peaks["source"],
+                         "fp64_tflops": w.flops_total / (ms / 1e3) / 1e12},
+            "clocks": clocks}
+    line.update(extra)
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_sample_extra(w, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del graph
+    torch.cuda.synchronize()
+    for hh in extra_handles:
+        hh.close()
+    handle.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def cpu_sample_extra(w, target_s):
+    """The oracle on the host cores for the extra rows: per-member gesv (variable size,
+    members split over threads by the oracle) or getrs with trans = T plus the rank-nrhs
+    product (adjoint), on a bounded sample."""
+    import oracle
+    threads = oracle.nthreads_default()
+    if w.name == "vbatched_4096":
+        if not hasattr(w, "host"):
+            w.host = (w.sizes.cpu().numpy(), w.rhs.cpu().numpy(), w.A0.cpu().numpy(),
+                      w.B0.cpu().numpy())
+        sz, kk, A0, B0 = w.host
+        t0 = time.perf_counter()
+        done = 0
+        while time.perf_counter() - t0 < target_s and done < w.bc:
+            b = done
+            n, k = int(sz[b]), int(kk[b])
+            A = np.ascontiguousarray(A0[b][:n, :n]).reshape(-1)  # column-major n x n, ld n
+            Bm = np.ascontiguousarray(B0[b][:k, :n]).reshape(-1)
+            ipiv = np.zeros(n, np.int32)
+            info = np.zeros(1, np.int32)
+            oracle.gesv(n, k, A, n, n * n, ipiv, n, Bm, n, n * k, info, 1, nthreads=1)
+            done += 1
+        t = time.perf_counter() - t0
+        return {"value": done / t, "unit": w.unit, "cores": 1, "kind": "port",
+                "sample": f"first {done} of {w.bc} members, oracle gesv one member per call "
+                          f"(1 thread), {t:.1f} s"}
+    n, nrhs = w.n, w.nrhs
+    cnt = min(w.bc, 2048)
+    A = w.A0[:cnt].cpu().numpy().reshape(-1).copy()
+    ipiv = np.zeros(cnt * n, np.int32)
+    info = np.zeros(cnt, np.int32)
+    oracle.getrf(n, n, A, n, n * n, ipiv, n, info, cnt, nthreads=threads)
+    X = w.X0[:cnt].cpu().numpy()
+    G = w.G0[:cnt].cpu().numpy().reshape(-1)
+    reps = 0
+    t0 = time.perf_counter()
+    while True:
+        gB = G.copy()
+        oracle.getrs(1, n, nrhs, A, n, n * n, ipiv, n, gB, n, n * nrhs, cnt, nthreads=threads)
+        gBm = gB.reshape(cnt, nrhs, n)
+        _ = -np.einsum("bcr,bcj->brj", gBm, X)
+        reps += 1
+        if time.perf_counter() - t0 >= target_s:
+            break
+    t = time.perf_counter() - t0
+    return {"value": reps * cnt / t, "unit": w.unit, "cores": threads, "kind": "port",
+            "sample": f"{cnt} of {w.bc} members x {reps}, oracle getrs (trans) with "
+                      f"{threads} pthreads + numpy outer product, {t:.1f} s"}
 
 
 if __name__ == "__main__":
