@@ -175,4 +175,68 @@ struct Scaler
     }
 };
 
+// ---------------------------------------------------------------------------------------
+// Rolled register rows (LU panels): the active column is register 0 and a rank-1 update
+// writes column c+1+i into register i.
+// Candidate rows are published shifted by one (dst[i] = v[i+1], dst[JB-1] = 0; the pivot
+// value itself goes to its own slot) with 16-byte vector stores, so that the rank-1
+// update, which pairs element i+1 of the pivot row with register i, reads aligned vectors.
+template <typename T, int JB>
+__device__ __forceinline__ void store_row_shifted(T* dst, const T (&v)[JB])
+{
+    auto at = [&](int i) { return i < JB ? v[i] : T(0); };
+    if constexpr(sizeof(T) == 8)
+    {
+#pragma unroll
+        for(int i = 0; i < JB; i += 2)
+            *reinterpret_cast<double2*>(dst + i) = make_double2(at(i + 1), at(i + 2));
+    }
+    else
+    {
+#pragma unroll
+        for(int i = 0; i < JB; i += 4)
+            *reinterpret_cast<float4*>(dst + i) =
+                make_float4(at(i + 1), at(i + 2), at(i + 3), at(i + 4));
+    }
+}
+// v[i] = fma(-l, row[i], v[i+1]) for i <= lim (and i < JB-1) with row read as aligned
+// vectors.  Registers above lim hold columns outside the panel; they are left stale, in
+// groups of 8 skipped by a branch that is uniform across the CTA (lim depends only on
+// the column).
+template <typename T, int JB>
+__device__ __forceinline__ void update_shift(T (&v)[JB], T l, const T* row, int lim)
+{
+#pragma unroll
+    for(int g = 0; g < JB; g += 8)
+    {
+        if(g > lim)
+            break;
+        if constexpr(sizeof(T) == 8)
+        {
+#pragma unroll
+            for(int i = g; i < g + 8 && i < JB; i += 2)
+            {
+                const double2 t = *reinterpret_cast<const double2*>(row + i);
+                if(i + 1 < JB)
+                    v[i] = fma(-l, t.x, v[i + 1]);
+                if(i + 2 < JB)
+                    v[i + 1] = fma(-l, t.y, v[i + 2]);
+            }
+        }
+        else
+        {
+#pragma unroll
+            for(int i = g; i < g + 8 && i < JB; i += 4)
+            {
+                const float4 t = *reinterpret_cast<const float4*>(row + i);
+                const float e[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                for(int u = 0; u < 4; ++u)
+                    if(i + u + 1 < JB)
+                        v[i + u] = fmaf(-l, e[u], v[i + u + 1]);
+            }
+        }
+    }
+}
+
 } // namespace rsb
