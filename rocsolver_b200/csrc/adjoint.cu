@@ -43,6 +43,7 @@ __global__ void __launch_bounds__(NT, 2)
     for(int c0 = 0; c0 < nrhs; c0 += NRC)
     {
         const int nc = min(NRC, nrhs - c0);
+#pragma unroll 4
         for(int e = threadIdx.x; e < n * NRC; e += NT)
         {
             const int i = e % n, c = e / n;

@@ -494,12 +494,25 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
         {
             const int ncol = min(cw, n - c0);
             const int ncp = (ncol + 31) & ~31;
-            for(int e = tid; e < JB * ncp; e += NT)
+            // loads of 4 elements issued before their stores (overlapped latency)
+            for(int e0 = tid; e0 < JB * ncp; e0 += 4 * NT)
             {
-                const int k = e % JB, col = e / JB;
-                sU[k * cwp + col] = (k < jb && col < ncol)
-                                        ? a[ix(j0 + (fold ? slotof[k] : k), c0 + col, lda)]
-                                        : T(0);
+                T t[4];
+#pragma unroll
+                for(int u = 0; u < 4; ++u)
+                {
+                    const int e = e0 + u * NT, k = e % JB, col = e / JB;
+                    t[u] = (e < JB * ncp && k < jb && col < ncol)
+                               ? a[ix(j0 + (fold ? slotof[k] : k), c0 + col, lda)]
+                               : T(0);
+                }
+#pragma unroll
+                for(int u = 0; u < 4; ++u)
+                {
+                    const int e = e0 + u * NT;
+                    if(e < JB * ncp)
+                        sU[(e % JB) * cwp + e / JB] = t[u];
+                }
             }
             __syncthreads();
             for(int t = warp; t < ncp / 32; t += NW)

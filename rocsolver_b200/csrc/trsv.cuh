@@ -51,27 +51,31 @@ template <typename T, bool LOWER>
 __device__ __forceinline__ void invert_block(bool unit, TriView<T> M, int kb, int nb, T* blk)
 {
     const int lane = threadIdx.x & 31;
-    for(int e = lane; e < 32 * 32; e += 32)
+    // 8 loads per lane issued before their stores (overlapped latency)
+    for(int e0 = lane; e0 < 32 * 32; e0 += 8 * 32)
     {
-        int i, k; // M's contiguous direction first
-        if(M.rs == 1)
+        T v[8];
+#pragma unroll
+        for(int u = 0; u < 8; ++u)
         {
-            i = e & 31;
-            k = e >> 5;
+            const int e = e0 + 32 * u;
+            const int i = M.rs == 1 ? (e & 31) : (e >> 5); // M's contiguous direction first
+            const int k = M.rs == 1 ? (e >> 5) : (e & 31);
+            if(i >= nb || k >= nb)
+                v[u] = i == k ? T(1) : T(0);
+            else if(i == k)
+                v[u] = unit ? T(1) : M(kb + i, kb + k);
+            else
+                v[u] = (LOWER ? i > k : i < k) ? M(kb + i, kb + k) : T(0);
         }
-        else
+#pragma unroll
+        for(int u = 0; u < 8; ++u)
         {
-            k = e & 31;
-            i = e >> 5;
+            const int e = e0 + 32 * u;
+            const int i = M.rs == 1 ? (e & 31) : (e >> 5);
+            const int k = M.rs == 1 ? (e >> 5) : (e & 31);
+            blk[i * SDIAG_LD + k] = v[u];
         }
-        T v;
-        if(i >= nb || k >= nb)
-            v = i == k ? T(1) : T(0);
-        else if(i == k)
-            v = unit ? T(1) : M(kb + i, kb + k);
-        else
-            v = (LOWER ? i > k : i < k) ? M(kb + i, kb + k) : T(0);
-        blk[i * SDIAG_LD + k] = v;
     }
     __syncwarp();
 #pragma unroll 1
@@ -302,6 +306,7 @@ __device__ __forceinline__ void getrs_dev(int trans, int n, int nrhs, const T* a
     for(int c0 = 0; c0 < nrhs; c0 += NRC)
     {
         const int nc = min(NRC, nrhs - c0);
+#pragma unroll 4
         for(int e = threadIdx.x; e < n * nc; e += NT)
         {
             const int i = e % n, c = e / n;
@@ -352,6 +357,7 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
     const bool pv = ipiv != nullptr;
     if(pv)
         build_perm(ipiv + b * strideP, n, perm);
+#pragma unroll 4
     for(int e = threadIdx.x; e < n * nc; e += NT)
     {
         const int i = e % n, c = e / n;
@@ -395,6 +401,7 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
         return;
     const T* a = A.at(b);
     T* x = B.at(b);
+#pragma unroll 4
     for(int e = threadIdx.x; e < n * nc; e += NT)
     {
         const int i = e % n, c = e / n;
@@ -443,12 +450,25 @@ __global__ void __launch_bounds__(N, N <= 32 ? 16 : 8)
     T* x = B.at(b);
     // L(i, j) = a[i + j*lda] (lower) or U(j, i) = a[j + i*lda] (upper); the fastest thread
     // index runs along the stored column either way
-    for(int e = r; e < N * N; e += N)
+    for(int e0 = r; e0 < N * N; e0 += 8 * N)
     {
-        const int p = e % N, q = e / N;
-        const int i = upper ? q : p, j = upper ? p : q; // L(i, j), i >= j
-        if(i < n && j <= i)
-            sL[i + j * LD] = upper ? a[ix(j, i, lda)] : a[ix(i, j, lda)];
+        T t[8];
+#pragma unroll
+        for(int u = 0; u < 8; ++u)
+        {
+            const int e = e0 + u * N, p = e % N, q = e / N;
+            const int i = upper ? q : p, j = upper ? p : q; // L(i, j), i >= j
+            t[u] = (e < N * N && i < n && j <= i) ? (upper ? a[ix(j, i, lda)] : a[ix(i, j, lda)])
+                                                  : T(0);
+        }
+#pragma unroll
+        for(int u = 0; u < 8; ++u)
+        {
+            const int e = e0 + u * N, p = e % N, q = e / N;
+            const int i = upper ? q : p, j = upper ? p : q;
+            if(e < N * N && i < n && j <= i)
+                sL[i + j * LD] = t[u];
+        }
     }
     T v[NRC];
 #pragma unroll
