@@ -43,13 +43,20 @@ __global__ void __launch_bounds__(NT, 2)
     for(int c0 = 0; c0 < nrhs; c0 += NRC)
     {
         const int nc = min(NRC, nrhs - c0);
-#pragma unroll 4
-        for(int e = threadIdx.x; e < n * NRC; e += NT)
-        {
-            const int i = e % n, c = e / n;
-            sg[e] = c < nc ? g[ix(i, c0 + c, ldg)] : T(0);
-            sx[e] = c < nc ? x[ix(i, c0 + c, ldx)] : T(0);
-        }
+        staged_copy<NT, 4>(
+            n * NRC,
+            [&](int e) {
+                const int i = e % n, c = e / n;
+                return c < nc ? g[ix(i, c0 + c, ldg)] : T(0);
+            },
+            [&](int e, T v) { sg[e] = v; });
+        staged_copy<NT, 4>(
+            n * NRC,
+            [&](int e) {
+                const int i = e % n, c = e / n;
+                return c < nc ? x[ix(i, c0 + c, ldx)] : T(0);
+            },
+            [&](int e, T v) { sx[e] = v; });
         __syncthreads();
         if(kind == 0)
         {

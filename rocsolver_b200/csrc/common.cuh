@@ -239,4 +239,31 @@ __device__ __forceinline__ void update_shift(T (&v)[JB], T l, const T* row, int 
     }
 }
 
+// Copy count elements into shared memory, store(e, load(e)) for e = threadIdx.x, +NT, ...,
+// with U loads per thread issued before their stores so that their latencies overlap
+// (a load feeding a shared-memory store otherwise waits for the previous store's load).
+template <int NT, int U, typename L, typename S>
+__device__ __forceinline__ void staged_copy(int count, L load, S store)
+{
+    using V = decltype(load(0));
+    for(int e0 = threadIdx.x; e0 < count; e0 += U * NT)
+    {
+        V t[U];
+#pragma unroll
+        for(int u = 0; u < U; ++u)
+        {
+            const int e = e0 + u * NT;
+            if(e < count)
+                t[u] = load(e);
+        }
+#pragma unroll
+        for(int u = 0; u < U; ++u)
+        {
+            const int e = e0 + u * NT;
+            if(e < count)
+                store(e, t[u]);
+        }
+    }
+}
+
 } // namespace rsb

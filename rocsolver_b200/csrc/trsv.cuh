@@ -306,13 +306,13 @@ __device__ __forceinline__ void getrs_dev(int trans, int n, int nrhs, const T* a
     for(int c0 = 0; c0 < nrhs; c0 += NRC)
     {
         const int nc = min(NRC, nrhs - c0);
-#pragma unroll 4
-        for(int e = threadIdx.x; e < n * nc; e += NT)
-        {
-            const int i = e % n, c = e / n;
-            const int src = (!trans && piv) ? perm[i] : i;
-            sb[i + c * n] = x[ix(src, c0 + c, ldb)];
-        }
+        staged_copy<NT, 4>(
+            n * nc,
+            [&](int e) {
+                const int i = e % n, c = e / n;
+                return x[ix((!trans && piv) ? perm[i] : i, c0 + c, ldb)];
+            },
+            [&](int e, T v) { sb[e] = v; });
         __syncthreads();
         if(!trans)
         {
@@ -357,13 +357,13 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
     const bool pv = ipiv != nullptr;
     if(pv)
         build_perm(ipiv + b * strideP, n, perm);
-#pragma unroll 4
-    for(int e = threadIdx.x; e < n * nc; e += NT)
-    {
-        const int i = e % n, c = e / n;
-        const int src = (!trans && pv) ? perm[i] : i;
-        sb[i + c * n] = x[ix(src, c0 + c, ldb)];
-    }
+    staged_copy<NT, 4>(
+        n * nc,
+        [&](int e) {
+            const int i = e % n, c = e / n;
+            return x[ix((!trans && pv) ? perm[i] : i, c0 + c, ldb)];
+        },
+        [&](int e, T v) { sb[e] = v; });
     __syncthreads();
     if(!trans)
     {
@@ -401,12 +401,9 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
         return;
     const T* a = A.at(b);
     T* x = B.at(b);
-#pragma unroll 4
-    for(int e = threadIdx.x; e < n * nc; e += NT)
-    {
-        const int i = e % n, c = e / n;
-        sb[i + c * n] = x[ix(i, c0 + c, ldb)];
-    }
+    staged_copy<NT, 4>(
+        n * nc, [&](int e) { return x[ix(e % n, c0 + e / n, ldb)]; },
+        [&](int e, T v) { sb[e] = v; });
     __syncthreads();
     if(!upper)
     {
