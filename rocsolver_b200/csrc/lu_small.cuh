@@ -25,7 +25,9 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
     getrf_warp_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
                       int bc, Gate gate)
 {
-    __shared__ T srow[SMALL_WPB][2][NMAX];
+    // pivot row, double-buffered; element NMAX holds the pivot's reciprocal.  Rows of
+    // NMAX + 4 elements keep every row 16-byte aligned for the vector accesses.
+    __shared__ __align__(16) T srow[SMALL_WPB][2][NMAX + 4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = (int64_t)blockIdx.x * SMALL_WPB + warp;
     if(b >= bc || gate.skip(b))
@@ -36,6 +38,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
     for(int j = 0; j < NMAX; ++j)
         r[j] = (lane < m && j < n) ? a[ix(lane, j, lda)] : T(0);
 
+    constexpr int VW = 16 / sizeof(T); // elements per 16-byte vector
     int myrow = lane;
     int mypiv = lane + 1;
     int inf = 0;
@@ -46,6 +49,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
         if(k < mn)
         {
             const int buf = k & 1;
+            T* row = srow[warp][buf];
             int prow = k;
             if(PIVOT)
             {
@@ -55,12 +59,24 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
             }
             if(myrow == prow)
             {
+                // publish columns from the vector boundary at or below k (the extra leading
+                // elements are never read) and the reciprocal of the pivot
 #pragma unroll
-                for(int j = k; j < NMAX; ++j)
-                    srow[warp][buf][j] = r[j];
+                for(int j = 0; j < NMAX; j += VW)
+                {
+                    if(j + VW <= k)
+                        continue;
+                    if constexpr(sizeof(T) == 8)
+                        *reinterpret_cast<double2*>(row + j) = make_double2(r[j], r[j + 1]);
+                    else
+                        *reinterpret_cast<float4*>(row + j) =
+                            make_float4(r[j], r[j + 1], r[j + 2], r[j + 3]);
+                }
+                row[NMAX] = r[k] != T(0) ? Lim<T>::rcp(r[k]) : T(0);
             }
             __syncwarp();
-            const T piv = srow[warp][buf][k];
+            const T piv = row[k];
+            const T rcp = row[NMAX];
             if(lane == k)
                 mypiv = prow + 1;
             if(piv == T(0) && inf == 0)
@@ -72,15 +88,38 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
                 else if(myrow == k)
                     myrow = prow;
             }
-            Scaler<T> s;
-            s.init(piv);
             if(lane < m && myrow > k)
             {
-                const T l = s.apply(r[k]);
+                // LAPACK getf2 scaling: reciprocal when |pivot| >= sfmin, else division
+                const int mode = piv == T(0) ? 0 : (fabs(piv) >= Lim<T>::sfmin() ? 1 : 2);
+                const T x = r[k];
+                const T l = mode == 1 ? x * rcp : (mode == 2 ? x / piv : x);
                 r[k] = l;
 #pragma unroll
-                for(int j = k + 1; j < NMAX; ++j)
-                    r[j] = fma(-l, srow[warp][buf][j], r[j]);
+                for(int j = 0; j < NMAX; j += VW)
+                {
+                    if(j + VW <= k)
+                        continue;
+                    T e[VW];
+                    if constexpr(sizeof(T) == 8)
+                    {
+                        const double2 t = *reinterpret_cast<const double2*>(row + j);
+                        e[0] = t.x;
+                        e[1] = t.y;
+                    }
+                    else
+                    {
+                        const float4 t = *reinterpret_cast<const float4*>(row + j);
+                        e[0] = t.x;
+                        e[1] = t.y;
+                        e[2] = t.z;
+                        e[3] = t.w;
+                    }
+#pragma unroll
+                    for(int u = 0; u < VW; ++u)
+                        if(j + u > k)
+                            r[j + u] = fma(-l, e[u], r[j + u]);
+                }
             }
         }
     }
