@@ -180,8 +180,8 @@ def build_workload(name, torch, rs, dev, handle):
         w.bytes_per_unit_getrf = 2 * n * n * 8 + 4 * n + 4
         w.dominant = "getrf_cta_kernel<double, 256, 1, 32>"
         # DRAM bytes per member of the dominant kernel, from one ncu capture at batch 512
-        # (profiles/getrf_cta_fp64_n256_b512.md: 1454.9 MB / 512)
-        w.traffic_per_unit = 1454932736 / 512
+        # (profiles/getrf_cta_fp64_n256_b512.md: 1443.0 MB / 512)
+        w.traffic_per_unit = 1443046400 / 512
         w.launches_per_step = 2
         if name == "dsgesv_n256":
             w.metric = ("batched solves/s at FP64 backward err <=1e-13: mixed+IR vs plain FP64 LU")
@@ -189,8 +189,8 @@ def build_workload(name, torch, rs, dev, handle):
                                     "fallback) vs plain dgetrf+dgetrs, n=256, batch=2048, nrhs=1, "
                                     "cond log-uniform [1e1,1e6]")
             w.dominant = "getrf_cta_kernel<float, 128, 2, 32> (FP32 LU inside dsgesv)"
-            # profiles/getrf_cta_fp32_n256_b512.md: 636.3 MB / 512
-            w.traffic_per_unit = 636258816 / 512
+            # profiles/getrf_cta_fp32_n256_b512.md: 624.9 MB / 512
+            w.traffic_per_unit = 624886528 / 512
             w.launches_per_step = 6
     elif name == "getrf_n32":
         n, bc, nrhs = 32, 1000, 1
@@ -214,7 +214,7 @@ def build_workload(name, torch, rs, dev, handle):
         # profiles/getrf_warp_fp64_n32_b1000.md captures one 8 MB batch, which stays in L2
         # under replay (8.3 MB / 1000); the bench rotates 24 copies so its traffic is the
         # algorithmic figure
-        w.traffic_per_unit = 8278784 / 1000
+        w.traffic_per_unit = 8269824 / 1000
         w.launches_per_step = 2
     elif name == "potrf_n64":
         n, bc, nrhs = 64, 20000, 4
@@ -237,8 +237,8 @@ def build_workload(name, torch, rs, dev, handle):
         w.flops_per_unit = n ** 3 / 3.0 + n * n / 2.0 + n / 6.0 + 2.0 * n * n * nrhs
         w.bytes_per_unit_getrf = 2 * (n * (n + 1) // 2) * 8 + 4  # triangle read+write + info
         w.dominant = "potrf_reg_kernel<double, 64>"
-        # profiles/potrf_reg_fp64_n64_b4000.md: 105.5 MB / 4000
-        w.traffic_per_unit = 105541632 / 4000
+        # profiles/potrf_reg_fp64_n64_b4000.md: 105.6 MB / 4000
+        w.traffic_per_unit = 105635840 / 4000
         w.launches_per_step = 2
     else:
         raise ValueError(name)
@@ -650,6 +650,9 @@ def _extra_workload(name, torch, dev):
         k = w.rhs.double()
         w.bytes_total = float((2 * n * n * 8 + 2 * n * k * 8 + 4 * n + 4).sum())
         w.flops_total = float((2 * n ** 3 / 3 + 2 * n * n * k).sum())
+        # DRAM bytes per member from one ncu capture of 512 members of the same
+        # distribution (profiles/vb_persistent_fp64_nmax512_b512.md: 7998.3 MB / 512)
+        w.traffic_per_unit = 7998267000 / 512
     else:
         w.bc, w.n, w.nrhs = 8192, 128, 8
         g = torch.Generator(device=dev)
@@ -669,6 +672,8 @@ def _extra_workload(name, torch, dev):
                     "l2": "factors 1 GiB > L2"}
         w.bytes_total = bc * (2 * n * n * 8 + 4 * n * nrhs * 8 + 4 * n)
         w.flops_total = bc * (4.0 * n * n * nrhs)
+        # profiles/solve_adjoint_fp64_n128_b1024.md: 245.5 MB / 1024
+        w.traffic_per_unit = 245479424 / 1024
     return w
 
 
@@ -896,7 +901,8 @@ def main_extra(args, rank, world, local):
             "roofline": {"bound": "hbm", "kernel": "vb_persistent_kernel<double>"
                          if w.name == "vbatched_4096" else "solve_adjoint_kernel<double>",
                          "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": gbs / peaks["hbm_gbs"], "traffic": None,
+                         "frac": gbs / peaks["hbm_gbs"],
+                         "traffic": w.traffic_per_unit * bc,
                          "peak_source": peaks["source"],
                          "fp64_tflops": w.flops_total / (ms / 1e3) / 1e12},
             "clocks": clocks}
