@@ -122,6 +122,7 @@ static rocblas_status run_getrf_tuned(const LuCfg& c, cudaStream_t s, int m, int
     RSB_LU_VARIANT(128, 4, 16)
     RSB_LU_VARIANT(256, 1, 32)
     RSB_LU_VARIANT(256, 2, 16)
+    RSB_LU_VARIANT(256, 2, 32)
     RSB_LU_VARIANT(256, 4, 8)
     RSB_LU_VARIANT(256, 8, 4)
 #undef RSB_LU_VARIANT

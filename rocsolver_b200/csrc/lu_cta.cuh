@@ -578,11 +578,12 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
 }
 
 // 128-thread CTAs: 3 per SM, or LU_MIN_BLOCKS_128 when the panel fits the smaller register
-// budget (FP32, or one row per thread)
+// budget (FP32, or one row per thread); 256-thread CTAs: LU_MIN_BLOCKS, or one per SM for
+// panels of more than 32 registers per thread (two rows of a 32-wide panel)
 template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
 __global__ void __launch_bounds__(NT,
                                   NT <= 128 ? ((sizeof(T) == 4 || R == 1) ? LU_MIN_BLOCKS_128 : 3)
-                                            : LU_MIN_BLOCKS)
+                                            : (R * JB > 32 ? 1 : LU_MIN_BLOCKS))
     getrf_cta_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
                      int cw, int fold, Gate gate)
 {

@@ -91,7 +91,7 @@ __device__ __forceinline__ bool vb_valid(const VbArgs& v, int b)
 }
 
 template <typename T, int NT, int R, int JB, int TN>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, R * JB > 32 ? 1 : 2)
     vb_persistent_kernel(VbArgs v, T* const* A, T* const* B, int cw, int fold)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -312,6 +312,8 @@ rocblas_status launch_vbatched(cudaStream_t s, int mode, const int* n, const int
             st = run_vb<T, 256, 1, 32, 8>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
         else if(c.r == 2 && c.jb == 16)
             st = run_vb<T, 256, 2, 16, 8>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
+        else if(c.r == 2 && c.jb == 32)
+            st = run_vb<T, 256, 2, 32, 8>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
         else if(c.r == 4 && c.jb == 8)
             st = run_vb<T, 256, 4, 8, 4>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
         else if(c.r == 8 && c.jb == 4)
