@@ -124,7 +124,9 @@ static rocblas_status run_getrf_tuned(const LuCfg& c, cudaStream_t s, int m, int
     RSB_LU_VARIANT(256, 2, 16)
     RSB_LU_VARIANT(256, 2, 32)
     RSB_LU_VARIANT(256, 4, 8)
+    RSB_LU_VARIANT(256, 4, 16)
     RSB_LU_VARIANT(256, 8, 4)
+    RSB_LU_VARIANT(256, 8, 8)
 #undef RSB_LU_VARIANT
     return rocblas_status_not_implemented;
 }

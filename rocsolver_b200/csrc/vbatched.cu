@@ -316,6 +316,8 @@ rocblas_status launch_vbatched(cudaStream_t s, int mode, const int* n, const int
             st = run_vb<T, 256, 2, 32, 8>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
         else if(c.r == 4 && c.jb == 8)
             st = run_vb<T, 256, 4, 8, 4>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
+        else if(c.r == 4 && c.jb == 16)
+            st = run_vb<T, 256, 4, 16, 8>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
         else if(c.r == 8 && c.jb == 4)
             st = run_vb<T, 256, 8, 4, 4>(s, v, A, B, c.cw, c.fold, c.per_sm, &ran);
         if(ran)

@@ -30,8 +30,10 @@ DEFAULT_OUT = os.path.join(HERE, "tuning_b200.txt")
 
 # compiled CTA variants: (threads, rows per thread, panel width)
 LU_VARIANTS = [(64, 1, 32), (128, 1, 32), (128, 2, 32), (128, 2, 16), (128, 4, 16),
-               (256, 1, 32), (256, 2, 16), (256, 2, 32), (256, 4, 8), (256, 8, 4)]
-VB_VARIANTS = [(256, 1, 32), (256, 2, 16), (256, 2, 32), (256, 4, 8), (256, 8, 4)]
+               (256, 1, 32), (256, 2, 16), (256, 2, 32), (256, 4, 8), (256, 4, 16),
+               (256, 8, 4), (256, 8, 8)]
+VB_VARIANTS = [(256, 1, 32), (256, 2, 16), (256, 2, 32), (256, 4, 8), (256, 4, 16),
+               (256, 8, 4)]
 # batch per getrf size class (enough CTAs for several waves on 148 SMs)
 GETRF_CLASSES = {64: 16384, 128: 8192, 256: 2048, 512: 592, 1024: 296, 2048: 148}
 VB_CLASSES = {256: 4096, 512: 4096, 1024: 1024}
