@@ -149,7 +149,7 @@ def tune_vbatched(prec, nmax, bc, reps, quick, log):
         for nt, r, jb in VB_VARIANTS:
             if nt * r < nmax or nt * r >= 4 * nmax:
                 continue
-            for cw in ((0,) if quick else (0, 64)):
+            for cw in ((0,) if quick else (32, 64, 128)):
                 for fold in (0, 1):
                     for per_sm in (0, 1):
                         cand = (nt, r, jb, cw, fold, per_sm)
