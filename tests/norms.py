@@ -1,5 +1,5 @@
 """Error metrics of the reference's test clients (clients/include/norm.hpp:16-112)
-and the backward errors the benchmarked configurations are judged by."""
+and the backward errors reported for the benchmarked configurations."""
 import numpy as np
 
 EPS = {np.float64: np.finfo(np.float64).eps, np.float32: np.finfo(np.float32).eps}
