@@ -651,8 +651,8 @@ def _extra_workload(name, torch, dev):
         w.bytes_total = float((2 * n * n * 8 + 2 * n * k * 8 + 4 * n + 4).sum())
         w.flops_total = float((2 * n ** 3 / 3 + 2 * n * n * k).sum())
         # DRAM bytes per member from one ncu capture of 512 members of the same
-        # distribution (profiles/vb_persistent_fp64_nmax512_b512.md: 7998.3 MB / 512)
-        w.traffic_per_unit = 7998267000 / 512
+        # distribution (profiles/vb_persistent_fp64_nmax512_b512.md: 4464.1 MB / 512)
+        w.traffic_per_unit = 4464067000 / 512
     else:
         w.bc, w.n, w.nrhs = 8192, 128, 8
         g = torch.Generator(device=dev)
