@@ -59,6 +59,17 @@ def parse():
     return p.parse_args()
 
 
+# ----------------------------------------------------------------------------- ranks
+def max_over_ranks(torch, pg, value, device):
+    """The largest value over all ranks (every rank's device time is reduced so that the
+    reported time is the slowest rank's); value itself without a process group."""
+    if pg is None:
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ----------------------------------------------------------------------------- peaks
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -527,15 +538,9 @@ def main():
     else:
         res = run_ours(w, torch, rs, dev, handle, args.steps, args.warmup)
     total_ms = sum(res["step_ms"])
-    if pg:
-        t = torch.tensor([total_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(torch, pg, total_ms, dev)
     e2e = run_e2e(w, torch, rs, dev, handle, args.steps)
-    if pg:
-        t = torch.tensor([e2e["ms"]], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e["ms"] = float(t.item())
+    e2e["ms"] = max_over_ranks(torch, pg, e2e["ms"], dev)
     ms_per_step = total_ms / args.steps
     units = w.bc * world
     value = units / (ms_per_step / 1e3)
@@ -774,10 +779,7 @@ def main_extra(args, rank, world, local):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     total_ms = sum(a.elapsed_time(b) for a, b in ev)
-    if pg:
-        t = torch.tensor([total_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(torch, pg, total_ms, dev)
     ms = total_ms / args.steps
     peaks = load_peaks()
     gbs = w.bytes_total / (ms / 1e3) / 1e9
@@ -887,10 +889,7 @@ def main_extra(args, rank, world, local):
     b2.record(stream)
     torch.cuda.synchronize()
     e2e_ms = a.elapsed_time(b2) / k
-    if pg:
-        t = torch.tensor([e2e_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(torch, pg, e2e_ms, dev)
     line = {"metric": w.metric, "value": bc * world / (ms / 1e3), "unit": w.unit,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
