@@ -24,6 +24,7 @@ configurations; no dataset is involved):
               dgetrs_batched per distinct n, "per_size_launches").
   adjoint_n128   n=128, batch 8192, nrhs 8, FP64, A ~ U[-1,1] + 4 I factored once outside
               the timing, G ~ N(0,1): rocsolver_dgetrs_adjoint_strided_batched (gB, gA).
+  adjoint_n128_fp32  the same in FP32 (rocsolver_sgetrs_adjoint_strided_batched).
 Inputs are larger than L2 (126 MB) for gesv_n256 and potrf_n64; getrf_n32 (8 MB) rotates
 through 24 distinct copies of the batch so each step reads cold data.
 
@@ -53,7 +54,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="dsgesv_n256",
                    choices=["dsgesv_n256", "gesv_n256", "getrf_n32", "potrf_n64",
-                            "vbatched_4096", "adjoint_n128"])
+                            "vbatched_4096", "adjoint_n128", "adjoint_n128_fp32"])
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target CPU time of the bounded CPU-baseline sample")
     return p.parse_args()
@@ -513,7 +514,7 @@ def main():
 
     if args.impl == "reference":
         return main_reference(args, rank, world)
-    if args.workload in ("vbatched_4096", "adjoint_n128"):
+    if args.workload in ("vbatched_4096", "adjoint_n128", "adjoint_n128_fp32"):
         return main_extra(args, rank, world, local)
 
     import torch
@@ -603,7 +604,7 @@ def main_reference(args, rank, world):
         return
     import torch
     dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
-    extra = args.workload in ("vbatched_4096", "adjoint_n128")
+    extra = args.workload in ("vbatched_4096", "adjoint_n128", "adjoint_n128_fp32")
     w = (_extra_workload(args.workload, torch, dev) if extra
          else build_workload(args.workload, torch, None, dev, None))
     w.dtype = getattr(w, "dtype", "f64")
@@ -660,25 +661,31 @@ def _extra_workload(name, torch, dev):
         w.traffic_per_unit = 4464067000 / 512
     else:
         w.bc, w.n, w.nrhs = 8192, 128, 8
+        w.prec = "s" if name.endswith("fp32") else "d"
+        dt = torch.float32 if w.prec == "s" else torch.float64
+        es = 4 if w.prec == "s" else 8
+        w.dtype = "f32" if w.prec == "s" else "f64"
         g = torch.Generator(device=dev)
         g.manual_seed(12)
         n, bc, nrhs = w.n, w.bc, w.nrhs
         A = torch.rand(bc, n, n, generator=g, device=dev, dtype=torch.float64) * 2 - 1
         A += 4 * torch.eye(n, device=dev, dtype=torch.float64)
         w.Arow = A
-        w.A0 = A.transpose(1, 2).contiguous()
-        w.X0 = torch.randn(bc, nrhs, n, generator=g, device=dev, dtype=torch.float64)
-        w.G0 = torch.randn(bc, nrhs, n, generator=g, device=dev, dtype=torch.float64)
-        w.metric = "batched solve adjoints/s (FP64 getrs_adjoint: gB = A^-T G, gA = -gB X')"
+        w.A0 = A.to(dt).transpose(1, 2).contiguous()
+        w.X0 = torch.randn(bc, nrhs, n, generator=g, device=dev, dtype=torch.float64).to(dt)
+        w.G0 = torch.randn(bc, nrhs, n, generator=g, device=dev, dtype=torch.float64).to(dt)
+        w.metric = (f"batched solve adjoints/s ({'FP32' if w.prec == 's' else 'FP64'} "
+                    f"getrs_adjoint: gB = A^-T G, gA = -gB X')")
         w.unit = "adjoints/s"
-        w.config = {"workload": "rocsolver_dgetrs_adjoint_strided_batched, n=128, batch 8192, "
-                                "nrhs 8, A ~ U[-1,1] + 4 I factored once (not timed), "
-                                "G ~ N(0,1)", "n": n, "batch": bc, "nrhs": nrhs,
-                    "l2": "factors 1 GiB > L2"}
-        w.bytes_total = bc * (2 * n * n * 8 + 4 * n * nrhs * 8 + 4 * n)
+        w.config = {"workload": f"rocsolver_{w.prec}getrs_adjoint_strided_batched, n=128, "
+                                "batch 8192, nrhs 8, A ~ U[-1,1] + 4 I factored once (not "
+                                "timed), G ~ N(0,1)", "n": n, "batch": bc, "nrhs": nrhs,
+                    "l2": f"factors {bc * n * n * es / 2**30:.1f} GiB > L2"}
+        w.bytes_total = bc * (2 * n * n * es + 4 * n * nrhs * es + 4 * n)
         w.flops_total = bc * (4.0 * n * n * nrhs)
-        # profiles/solve_adjoint_fp64_n128_b1024.md: 245.5 MB / 1024
-        w.traffic_per_unit = 245479424 / 1024
+        # profiles/solve_adjoint_fp64_n128_b1024.md: 245.5 MB / 1024 (FP64; FP32 scaled by
+        # the element size)
+        w.traffic_per_unit = 245479424 / 1024 * es / 8
     return w
 
 
@@ -745,13 +752,13 @@ def main_extra(args, rank, world, local):
         LU = w.A0.clone()
         ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
         info = torch.zeros(bc, dtype=torch.int32, device=dev)
-        rs.check(rs.call("rocsolver_dgetrf_strided_batched", h, n, n, P(LU), n, n * n, P(ipiv),
-                         n, P(info), bc), "getrf")
+        rs.check(rs.call(f"rocsolver_{w.prec}getrf_strided_batched", h, n, n, P(LU), n, n * n,
+                         P(ipiv), n, P(info), bc), "getrf")
         gA = torch.empty_like(LU)
         gB = torch.empty_like(w.G0)
 
         def call():
-            rs.check(rs.call("rocsolver_dgetrs_adjoint_strided_batched", h, n, nrhs, P(LU), n,
+            rs.check(rs.call(f"rocsolver_{w.prec}getrs_adjoint_strided_batched", h, n, nrhs, P(LU), n,
                              n * n, P(ipiv), n, P(w.X0), n, n * nrhs, P(w.G0), n, n * nrhs,
                              P(gA), n, n * n, P(gB), n, n * nrhs, bc), "adjoint")
 
@@ -851,13 +858,14 @@ def main_extra(args, rank, world, local):
         call()
         torch.cuda.synchronize()
         # gB against A^{-T} G and gA against -gB X' computed with torch (FP64)
-        Gt = w.G0.transpose(1, 2)
-        gBt = gB.transpose(1, 2)
-        res = torch.bmm(w.Arow.transpose(1, 2), gBt) - Gt
-        rel_b = float((res.abs().amax((1, 2)) / (w.Arow.abs().sum(1).amax(1)
+        Gt = w.G0.double().transpose(1, 2)
+        gBt = gB.double().transpose(1, 2)
+        Aw = w.A0.double().transpose(1, 2)  # the matrix as factored (rounded for FP32)
+        res = torch.bmm(Aw.transpose(1, 2), gBt) - Gt
+        rel_b = float((res.abs().amax((1, 2)) / (Aw.abs().sum(1).amax(1)
                                                  * gBt.abs().amax((1, 2)))).max())
-        gA_ref = -torch.bmm(gBt, w.X0)
-        rel_a = float(((gA.transpose(1, 2) - gA_ref).abs().amax((1, 2))
+        gA_ref = -torch.bmm(gBt, w.X0.double())
+        rel_a = float(((gA.double().transpose(1, 2) - gA_ref).abs().amax((1, 2))
                        / gA_ref.abs().amax((1, 2))).max())
         extra["accuracy"] = {"gB_backward_err_max": rel_b, "gA_rel_err_max": rel_a}
         hLU, hP = LU.cpu().pin_memory(), ipiv.cpu().pin_memory()
@@ -871,13 +879,14 @@ def main_extra(args, rank, world, local):
             dP.copy_(hP, non_blocking=True)
             dX.copy_(hX, non_blocking=True)
             dG.copy_(hG, non_blocking=True)
-            rs.check(rs.call("rocsolver_dgetrs_adjoint_strided_batched", h, n, nrhs, P(dLU), n,
+            rs.check(rs.call(f"rocsolver_{w.prec}getrs_adjoint_strided_batched", h, n, nrhs, P(dLU), n,
                              n * n, P(dP), n, P(dX), n, n * nrhs, P(dG), n, n * nrhs, P(gA), n,
                              n * n, P(gB), n, n * nrhs, bc), "adjoint")
             hgA.copy_(gA, non_blocking=True)
             hgB.copy_(gB, non_blocking=True)
-        h2d = (hLU.numel() + hX.numel() + hG.numel()) * 8 + hP.numel() * 4
-        d2h = (hgA.numel() + hgB.numel()) * 8
+        es = LU.element_size()
+        h2d = (hLU.numel() + hX.numel() + hG.numel()) * es + hP.numel() * 4
+        d2h = (hgA.numel() + hgB.numel()) * es
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
@@ -892,13 +901,15 @@ def main_extra(args, rank, world, local):
     e2e_ms = max_over_ranks(torch, pg, e2e_ms, dev)
     line = {"metric": w.metric, "value": bc * world / (ms / 1e3), "unit": w.unit,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": getattr(w, "dtype", "f64"),
             "data": "synthetic (seeded, generated on device)", "config": w.config,
             "gpu_launches": launches * args.steps,
             "e2e": {"value": bc * world / (e2e_ms / 1e3), "unit": w.unit,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "kernel": "vb_persistent_kernel<double>"
-                         if w.name == "vbatched_4096" else "solve_adjoint_kernel<double>",
+                         if w.name == "vbatched_4096" else
+                         f"solve_adjoint_kernel<{'float' if w.prec == 's' else 'double'}>",
                          "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": gbs / peaks["hbm_gbs"],
                          "traffic": w.traffic_per_unit * bc,
@@ -948,12 +959,12 @@ def cpu_sample_extra(w, target_s):
                           f"(1 thread), {t:.1f} s"}
     n, nrhs = w.n, w.nrhs
     cnt = min(w.bc, 2048)
-    A = w.A0[:cnt].cpu().numpy().reshape(-1).copy()
+    A = w.A0[:cnt].double().cpu().numpy().reshape(-1).copy()
     ipiv = np.zeros(cnt * n, np.int32)
     info = np.zeros(cnt, np.int32)
     oracle.getrf(n, n, A, n, n * n, ipiv, n, info, cnt, nthreads=threads)
-    X = w.X0[:cnt].cpu().numpy()
-    G = w.G0[:cnt].cpu().numpy().reshape(-1)
+    X = w.X0[:cnt].double().cpu().numpy()
+    G = w.G0[:cnt].double().cpu().numpy().reshape(-1)
     reps = 0
     t0 = time.perf_counter()
     while True:
