@@ -138,25 +138,20 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
 
 // Source-row map of the row interchanges ipiv[0..n-1]: after applying the swaps in order
 // (LAPACK dlaswp, incx = 1) position i holds original row src (returned for lane i).
+// Interchange k maps a'[i] = a[f_k(i)] with f_k the transposition (k, ipiv[k]-1), so
+// src(i) = f_0(f_1(...f_{n-1}(i))): each lane composes the transpositions for its own
+// position, one broadcast pivot per step (no serial chain of dependent shuffles).
 __device__ __forceinline__ int warp_perm_src(const int* piv, int n, int lane)
 {
     const unsigned full = 0xffffffffu;
-    int pv = lane < n ? piv[lane] - 1 : lane;
-    int src = lane;
-    for(int k = 0; k < n; ++k)
+    const int pv = lane < n ? piv[lane] - 1 : lane;
+    int x = lane;
+    for(int k = n - 1; k >= 0; --k)
     {
-        int p = __shfl_sync(full, pv, k);
-        if(p != k)
-        {
-            int vk = __shfl_sync(full, src, k);
-            int vp = __shfl_sync(full, src, p);
-            if(lane == k)
-                src = vp;
-            else if(lane == p)
-                src = vk;
-        }
+        const int p = __shfl_sync(full, pv, k);
+        x = x == k ? p : (x == p ? k : x);
     }
-    return src;
+    return (x >= 0 && x < n) ? x : lane;
 }
 
 // getrs for n <= NMAX <= 32 (library/src/lapack/roclapack_getrs.hpp:117-150 order:
@@ -186,6 +181,15 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
     for(int j = 0; j < NMAX; ++j)
         r[j] = (lane < n && j < n) ? (trans ? a[ix(j, lane, lda)] : a[ix(lane, j, lda)]) : T(0);
     const int src = ipiv ? warp_perm_src(ipiv + b * strideP, n, lane) : lane;
+    // reciprocal of this lane's diagonal entry U(lane, lane), computed off the sweeps'
+    // serial path (the sweeps multiply by it, as the reference's trsm applies inverted
+    // diagonal blocks)
+    T diag = T(1);
+#pragma unroll
+    for(int j = 0; j < NMAX; ++j)
+        if(j == lane)
+            diag = r[j];
+    const T rdiag = T(1) / diag;
 
     T v[NRC];
 #pragma unroll
@@ -219,7 +223,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
                 for(int c = 0; c < NRC; ++c)
                 {
                     if(lane == k)
-                        v[c] = v[c] / r[k];
+                        v[c] = v[c] * rdiag;
                     T xk = __shfl_sync(full, v[c], k);
                     if(lane < k)
                         v[c] = fma(-r[k], xk, v[c]);
@@ -239,7 +243,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
                 for(int c = 0; c < NRC; ++c)
                 {
                     if(lane == k)
-                        v[c] = v[c] / r[k];
+                        v[c] = v[c] * rdiag;
                     T yk = __shfl_sync(full, v[c], k);
                     if(lane > k)
                         v[c] = fma(-r[k], yk, v[c]);
