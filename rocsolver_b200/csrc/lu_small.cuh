@@ -342,6 +342,13 @@ __device__ __forceinline__ void gesv_warp_dev(int n, int nrhs, T* a, int lda, in
     if(inf != 0)
         return; // uniform: B stays untouched
     __syncwarp();
+    // reciprocal of this lane's diagonal entry U(myrow, myrow), off the serial path
+    T diag = T(1);
+#pragma unroll
+    for(int j = 0; j < NMAX; ++j)
+        if(j == myrow)
+            diag = r[j];
+    const T rdiag = T(1) / diag;
     for(int c0 = 0; c0 < nrhs; c0 += NRC)
     {
         // lane holds original row `lane` of B, which is position myrow of P*B
@@ -374,7 +381,7 @@ __device__ __forceinline__ void gesv_warp_dev(int n, int nrhs, T* a, int lda, in
                 for(int c = 0; c < NRC; ++c)
                 {
                     if(lane == o)
-                        v[c] = v[c] / r[k];
+                        v[c] = v[c] * rdiag;
                     T xk = __shfl_sync(full, v[c], o);
                     if(lane < n && myrow < k)
                         v[c] = fma(-r[k], xk, v[c]);
