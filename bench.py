@@ -200,9 +200,10 @@ def build_workload(name, torch, rs, dev, handle):
             w.config["workload"] = ("dsgesv_strided_batched (FP32 LU + FP64 IR, <=10 iters, FP64 "
                                     "fallback) vs plain dgetrf+dgetrs, n=256, batch=2048, nrhs=1, "
                                     "cond log-uniform [1e1,1e6]")
-            w.dominant = "getrf_cta_kernel<float, 128, 2, 32> (FP32 LU inside dsgesv)"
-            # profiles/getrf_cta_fp32_n256_b512.md: 624.9 MB / 512
-            w.traffic_per_unit = 624886528 / 512
+            w.dominant = ("getrf_cta_kernel<float, 128, 2, 32, TF32> (FP32 LU with split-TF32 "
+                          "tensor-core trailing updates inside dsgesv)")
+            # profiles/getrf_cta_tf32_n256_b512.md: 712.4 MB / 512
+            w.traffic_per_unit = 712355840 / 512
             w.launches_per_step = 6
     elif name == "getrf_n32":
         n, bc, nrhs = 32, 1000, 1
@@ -379,15 +380,16 @@ def run_mixed(w, torch, rs, dev, handle, steps, warmup):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    # FP32 LU kernel alone (the same kernel dsgesv launches), for the roofline
+    # FP32 LU kernel alone (the same kernel dsgesv launches, through its entry point), for
+    # the roofline
     A32 = w.A0.float()
     fev = []
     for _ in range(min(steps, 10)):
         Ac = A32.clone()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        rs.check(rs.call("rocsolver_sgetrf_strided_batched", h, n, n, rs.ptr(Ac), n, n * n,
-                         rs.ptr(ipiv), n, rs.ptr(info), bc), "sgetrf")
+        rs.check(rs.call("rocsolver_sgetrf_tf32_strided_batched", h, n, n, rs.ptr(Ac), n,
+                         n * n, rs.ptr(ipiv), n, rs.ptr(info), bc), "sgetrf_tf32")
         b.record(stream)
         fev.append((a, b))
     torch.cuda.synchronize()

@@ -582,6 +582,23 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dposv_strided_batched(rocblas_handle h
 
 /* ---- entry points with no counterpart in the reference ------------------ */
 
+/* FP32 LU with partial pivoting for a strided batch whose trailing updates run on the
+ * tensor cores as split-TF32 products (each operand split into two TF32 parts, three
+ * products accumulated in FP32: FP32-level accuracy, rounding not identical to
+ * rocsolver_sgetrf_strided_batched, so near-tied pivots may differ).  Arguments, ipiv and
+ * info as rocsolver_sgetrf_strided_batched (library/src/lapack/roclapack_getrf.cpp).  This
+ * is the factorisation rocsolver_dsgesv_strided_batched runs on its FP32 copy of A. */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetrf_tf32_strided_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
 /* Mixed-precision solver with iterative refinement for a strided batch (LAPACK dsgesv
  * semantics per member; the reference has no mixed-precision gesv).  Each member is
  * factored in FP32 (LU with partial pivoting of an FP32 copy of A), then refined in FP64:

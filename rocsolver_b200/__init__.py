@@ -74,6 +74,7 @@ for _p in "sd":
     _EXTRA[f"rocsolver_{_p}getrf_vbatched"] = (_c.c_int, [H, P, P, P, P, P, I, I])
     _EXTRA[f"rocsolver_{_p}getrs_vbatched"] = (_c.c_int, [H, P, P, P, P, P, P, P, I, I, I])
     _EXTRA[f"rocsolver_{_p}gesv_vbatched"] = (_c.c_int, [H, P, P, P, P, P, P, P, P, I, I, I])
+_EXTRA["rocsolver_sgetrf_tf32_strided_batched"] = (_c.c_int, [H, I, I, P, I, S, P, S, P, I])
 _EXTRA["rocsolver_dgesv_vbatched_noalloc"] = (_c.c_int, [H, P, P, P, P, P, P, P, P, I, I, I])
 _EXTRA["rocsolver_b200_tuning_set"] = (_c.c_int, [_c.c_char_p])
 _EXTRA["rocsolver_b200_tuning_load"] = (_c.c_int, [_c.c_char_p])

@@ -27,7 +27,8 @@ inline bool bad_fill(rocblas_fill f)
 
 template <typename T>
 rocblas_status getrf_impl(rocblas_handle h, int m, int n, Batch<T> A, const void* Aptr, int lda,
-                          int* ipiv, int64_t strideP, int* info, int bc, bool pivot)
+                          int* ipiv, int64_t strideP, int* info, int bc, bool pivot,
+                          bool tc = false)
 {
     if(!h)
         return rocblas_status_invalid_handle;
@@ -42,7 +43,8 @@ rocblas_status getrf_impl(rocblas_handle h, int m, int n, Batch<T> A, const void
         return rocblas_status_success;
     if(m == 0 || n == 0)
         return launch_reset_info(h->stream, info, bc);
-    return launch_getrf<T>(h->stream, m, n, A, lda, ipiv, strideP, info, bc, pivot);
+    return launch_getrf<T>(h->stream, m, n, A, lda, ipiv, strideP, info, bc, pivot, no_gate(),
+                           tc);
 }
 
 template <typename T>
@@ -301,6 +303,17 @@ extern "C" rocblas_status rocsolver_dsgesv_strided_batched(
 {
     return dsgesv_impl(handle, n, nrhs, A, lda, strideA, ipiv, strideP, B, ldb, strideB, X, ldx,
                        strideX, iter, info, batch_count);
+}
+
+// FP32 LU with split-TF32 tensor-core trailing updates (the factorisation of dsgesv);
+// argument checks as getrf (lapack/roclapack_getrf_strided_batched.cpp:8-84)
+extern "C" rocblas_status rocsolver_sgetrf_tf32_strided_batched(
+    rocblas_handle handle, const rocblas_int m, const rocblas_int n, float* A,
+    const rocblas_int lda, const rocblas_stride strideA, rocblas_int* ipiv,
+    const rocblas_stride strideP, rocblas_int* info, const rocblas_int batch_count)
+{
+    return getrf_impl<float>(handle, m, n, strided<float>(A, strideA), A, lda, ipiv, strideP,
+                             info, batch_count, true, true);
 }
 
 #define RSB_API_TYPE(P, T)                                                                      \

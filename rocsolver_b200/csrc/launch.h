@@ -12,10 +12,11 @@ namespace rsb {
 
 // Every launcher returns success, not_implemented (size outside the supported range)
 // or internal_error (launch failure).  None synchronises or allocates.
+// tc (FP32 with pivoting only): trailing updates as split-TF32 tensor products
 template <typename T>
 rocblas_status launch_getrf(cudaStream_t s, int m, int n, Batch<T> A, int lda, int* ipiv,
                             int64_t strideP, int* info, int bc, bool pivot,
-                            Gate gate = no_gate());
+                            Gate gate = no_gate(), bool tc = false);
 template <typename T>
 rocblas_status launch_getrs(cudaStream_t s, int trans, int n, int nrhs, Batch<T> A, int lda,
                             const int* ipiv, int64_t strideP, Batch<T> B, int ldb,

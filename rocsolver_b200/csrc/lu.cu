@@ -76,7 +76,7 @@ static void run_getrf_warp(cudaStream_t s, int m, int n, Batch<T> A, int lda, in
 // most, so that two CTAs fit in an SM's shared memory).  *ran = false when the variant
 // cannot take this size (more rows than threads x rows per thread, or too much shared
 // memory): the caller then uses the built-in choice.
-template <typename T, int NT, int R, int JB, bool PIVOT>
+template <typename T, int NT, int R, int JB, bool PIVOT, bool TC = false>
 static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, int lda,
                                     int* ipiv, int64_t sP, int* info, int bc, Gate g, int cw,
                                     int fold, bool* ran = nullptr)
@@ -95,7 +95,7 @@ static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, in
     const size_t smem = CtaLuSmem<T, NT, JB>::bytes(m, cw, R);
     if(smem > 227 * 1024)
         return rocblas_status_not_implemented;
-    auto k = getrf_cta_kernel<T, NT, R, JB, 8, PIVOT>;
+    auto k = getrf_cta_kernel<T, NT, R, JB, 8, PIVOT, TC>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
     if(ran)
@@ -105,7 +105,7 @@ static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, in
 }
 
 // the compiled CTA variants a tuning entry may name: (threads, rows per thread, panel width)
-template <typename T, bool PIVOT>
+template <typename T, bool PIVOT, bool TC>
 static rocblas_status run_getrf_tuned(const LuCfg& c, cudaStream_t s, int m, int n,
                                       Batch<T> A, int lda, int* ipiv, int64_t sP, int* info,
                                       int bc, Gate g, bool* ran)
@@ -113,8 +113,8 @@ static rocblas_status run_getrf_tuned(const LuCfg& c, cudaStream_t s, int m, int
     *ran = false;
 #define RSB_LU_VARIANT(NT_, R_, JB_)                                                          \
     if(c.nt == NT_ && c.r == R_ && c.jb == JB_)                                                \
-        return run_getrf_cta<T, NT_, R_, JB_, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g,  \
-                                                     c.cw, c.fold, ran);
+        return run_getrf_cta<T, NT_, R_, JB_, PIVOT, TC>(s, m, n, A, lda, ipiv, sP, info, bc, \
+                                                         g, c.cw, c.fold, ran);
     RSB_LU_VARIANT(64, 1, 32)
     RSB_LU_VARIANT(128, 1, 32)
     RSB_LU_VARIANT(128, 2, 32)
@@ -131,7 +131,7 @@ static rocblas_status run_getrf_tuned(const LuCfg& c, cudaStream_t s, int m, int
     return rocblas_status_not_implemented;
 }
 
-template <typename T, bool PIVOT>
+template <typename T, bool PIVOT, bool TC>
 static rocblas_status getrf_dispatch(cudaStream_t s, int m, int n, Batch<T> A, int lda,
                                      int* ipiv, int64_t sP, int* info, int bc, Gate g)
 {
@@ -150,36 +150,46 @@ static rocblas_status getrf_dispatch(cudaStream_t s, int m, int n, Batch<T> A, i
     {
         bool ran = false;
         const rocblas_status st =
-            run_getrf_tuned<T, PIVOT>(c, s, m, n, A, lda, ipiv, sP, info, bc, g, &ran);
+            run_getrf_tuned<T, PIVOT, TC>(c, s, m, n, A, lda, ipiv, sP, info, bc, g, &ran);
         if(ran)
             return st;
     }
     // built-in choice (used when no tuning table is installed)
     if(m <= 64)
-        return run_getrf_cta<T, 64, 1, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
+        return run_getrf_cta<T, 64, 1, 32, PIVOT, TC>(s, m, n, A, lda, ipiv, sP, info, bc,
+                                                   g, 0, 0);
     if(m <= 128)
-        return run_getrf_cta<T, 128, 1, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
+        return run_getrf_cta<T, 128, 1, 32, PIVOT, TC>(s, m, n, A, lda, ipiv, sP, info, bc,
+                                                   g, 0, 0);
     // FP32: 128-thread CTAs with two rows per thread (three CTAs per SM); FP64 keeps
     // 256 threads (its two-row panel would not fit the register budget)
     if(sizeof(T) == 4 && m <= 256)
-        return run_getrf_cta<T, 128, 2, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
+        return run_getrf_cta<T, 128, 2, 32, PIVOT, TC>(s, m, n, A, lda, ipiv, sP, info, bc,
+                                                   g, 0, 0);
     if(m <= 256)
-        return run_getrf_cta<T, 256, 1, 32, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
+        return run_getrf_cta<T, 256, 1, 32, PIVOT, TC>(s, m, n, A, lda, ipiv, sP, info, bc,
+                                                   g, 0, 0);
     if(m <= 512)
-        return run_getrf_cta<T, 256, 2, 16, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
+        return run_getrf_cta<T, 256, 2, 16, PIVOT, TC>(s, m, n, A, lda, ipiv, sP, info, bc,
+                                                   g, 0, 0);
     if(m <= 1024)
-        return run_getrf_cta<T, 256, 4, 8, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
+        return run_getrf_cta<T, 256, 4, 8, PIVOT, TC>(s, m, n, A, lda, ipiv, sP, info, bc,
+                                                   g, 0, 0);
     if(m <= MAX_CTA_ROWS)
-        return run_getrf_cta<T, 256, 8, 4, PIVOT>(s, m, n, A, lda, ipiv, sP, info, bc, g, 0, 0);
+        return run_getrf_cta<T, 256, 8, 4, PIVOT, TC>(s, m, n, A, lda, ipiv, sP, info, bc,
+                                                   g, 0, 0);
     return rocblas_status_not_implemented;
 }
 
 template <typename T>
 rocblas_status launch_getrf(cudaStream_t s, int m, int n, Batch<T> A, int lda, int* ipiv,
-                            int64_t sP, int* info, int bc, bool pivot, Gate g)
+                            int64_t sP, int* info, int bc, bool pivot, Gate g, bool tc)
 {
-    return pivot ? getrf_dispatch<T, true>(s, m, n, A, lda, ipiv, sP, info, bc, g)
-                 : getrf_dispatch<T, false>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+    if constexpr(sizeof(T) == 4)
+        if(tc && pivot)
+            return getrf_dispatch<T, true, true>(s, m, n, A, lda, ipiv, sP, info, bc, g);
+    return pivot ? getrf_dispatch<T, true, false>(s, m, n, A, lda, ipiv, sP, info, bc, g)
+                 : getrf_dispatch<T, false, false>(s, m, n, A, lda, ipiv, sP, info, bc, g);
 }
 
 // ------------------------------------------------------------------------------ getrs
@@ -384,7 +394,7 @@ rocblas_status launch_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T>
 // ------------------------------------------------------------------------------ instances
 #define RSB_INST(T)                                                                          \
     template rocblas_status launch_getrf<T>(cudaStream_t, int, int, Batch<T>, int, int*,   \
-                                            int64_t, int*, int, bool, Gate);               \
+                                            int64_t, int*, int, bool, Gate, bool);         \
     template rocblas_status launch_getrs<T>(cudaStream_t, int, int, int, Batch<T>, int,    \
                                             const int*, int64_t, Batch<T>, int, const int*, \
                                             int, Gate);                                    \

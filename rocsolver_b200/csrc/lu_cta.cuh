@@ -23,7 +23,8 @@
 //   * A22 -= L21 U12 as 32x32 warp tiles; A22 is streamed from L2/HBM once per panel.
 //   FP64 tiles run on the FP64 tensor path (mma.sync.m8n8k4.f64, 256 FMAs per instruction;
 //   tcgen05 has no FP64 kind); FP32 tiles are 4x8 register tiles per lane updated with
-//   packed fma.rn.f32x2 (two FMAs per instruction).  Shared-memory
+//   packed fma.rn.f32x2 (two FMAs per instruction), or, for the mixed solver, split-TF32
+//   tensor products (WarpTileTF32).  Shared-memory
 //   operands have leading dimension = 4 (mod 16) elements (bank-conflict-free fragments).
 #pragma once
 
@@ -204,12 +205,137 @@ struct WarpTile<float>
     }
 };
 
+// Round to TF32 (nearest, ties away from zero): half a TF32 unit added to the magnitude
+// bits, the 13 low mantissa bits cleared.  Integer operations only (the conversion
+// instruction runs on the narrow transcendental pipe).  Finite inputs near the FP32 limit
+// round to infinity, as the conversion does.
+__device__ __forceinline__ uint32_t tf32_rna(float x)
+{
+    return (__float_as_uint(x) + 0x1000u) & 0xffffe000u;
+}
+
+// x = hi + lo + O(2^-24 |x|): hi = x rounded to TF32, lo = (x - hi) (exact in FP32) rounded
+// to TF32
+__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo)
+{
+    hi = tf32_rna(x);
+    lo = tf32_rna(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1)
+{
+    asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 "
+        "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// FP32 tile product on the TF32 tensor path at FP32-level accuracy (split TF32, three
+// products): a = a_hi + a_lo, b = b_hi + b_lo, a*b ~ a_lo*b_hi + a_hi*b_lo + a_hi*b_hi
+// accumulated in FP32 (the dropped a_lo*b_lo is below 2^-21 |a||b|).  A 32 x 32 warp tile
+// is 2 x 4 blocks of mma.sync.m16n8k8 .tf32 (lane = 4*g + q holds rows g, g+8 of each
+// 16-row block and columns 2q, 2q+1 of each 8-column block); per 8-deep k step a lane
+// loads 16 operands (bank-conflict-free with leading dimensions = 4 mod 32) for 24 tensor
+// instructions, against 128 packed FMAs for the same step on CUDA cores.  Used for the
+// trailing update of the mixed solver's FP32 factorisation, where accuracy only sets the
+// refinement's convergence rate.
+struct WarpTileTF32
+{
+    float acc[2][4][4]; // [16-row block][8-column block][fragment element]
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for(int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for(int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for(int e = 0; e < 4; ++e)
+                    acc[mi][ni][e] = 0.f;
+    }
+    // arow[2*mi + h]: shared-memory row of tile row 16*mi + 8*h + g (see frag_row)
+    template <int K>
+    __device__ __forceinline__ void mma(const float* sA, int lda_s, const int (&arow)[4],
+                                        const float* sB, int ldb_s, int c0)
+    {
+        static_assert(K % 8 == 0, "TF32 k step is 8");
+        const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+#pragma unroll 1
+        for(int k0 = 0; k0 < K; k0 += 8)
+        {
+            uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
+            // A fragment element e: row g + 8*(e&1), k q + 4*(e>>1)
+#pragma unroll
+            for(int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for(int e = 0; e < 4; ++e)
+                    tf32_split(sA[(k0 + q + 4 * (e >> 1)) * lda_s + arow[mi * 2 + (e & 1)]],
+                               ah[mi][e], al[mi][e]);
+            // B fragment element e: k q + 4*e, column g
+#pragma unroll
+            for(int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for(int e = 0; e < 2; ++e)
+                    tf32_split(sB[(k0 + q + 4 * e) * ldb_s + c0 + ni * 8 + g], bh[ni][e],
+                               bl[ni][e]);
+            // small products first; eight independent blocks between dependent products
+#pragma unroll
+            for(int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for(int ni = 0; ni < 4; ++ni)
+                    mma_tf32(acc[mi][ni], al[mi], bh[ni][0], bh[ni][1]);
+#pragma unroll
+            for(int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for(int ni = 0; ni < 4; ++ni)
+                    mma_tf32(acc[mi][ni], ah[mi], bl[ni][0], bl[ni][1]);
+#pragma unroll
+            for(int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for(int ni = 0; ni < 4; ++ni)
+                    mma_tf32(acc[mi][ni], ah[mi], bh[ni][0], bh[ni][1]);
+        }
+    }
+    // accumulator element e of block (mi, ni): row 16*mi + g + 8*(e>>1), column
+    // 8*ni + 2*q + (e&1)
+    template <typename F>
+    __device__ __forceinline__ void each(F f)
+    {
+        const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+#pragma unroll
+        for(int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for(int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for(int e = 0; e < 4; ++e)
+                    f(mi * 16 + g + 8 * (e >> 1), ni * 8 + 2 * q + (e & 1), acc[mi][ni][e]);
+    }
+    static __device__ __forceinline__ int frag_row(int i)
+    {
+        return (i >> 1) * 16 + (i & 1) * 8 + ((threadIdx.x & 31) >> 2);
+    }
+};
+
+// tile type of the trailing update: TC selects the split-TF32 tensor path for FP32
+// (panel widths that are multiples of the 8-deep TF32 k step)
+template <typename T, bool TC>
+struct TileOf
+{
+    using type = WarpTile<T>;
+};
+template <>
+struct TileOf<float, true>
+{
+    using type = WarpTileTF32;
+};
+
 // Factor one m x n matrix with the whole CTA.  smem_raw must hold CtaLuSmem::bytes(m, cw, R);
 // m <= R*NT; cw is a multiple of 32.  Writes ipiv (1-based, PIVOT only) and *info_out.
 // fold: apply each panel's row interchanges to the columns right of it inside the trailing
 // update instead of swapping them in memory first (a tuning choice; same results).
+// TC: FP32 trailing products on the split-TF32 tensor path (WarpTileTF32).
 // Called by all threads of the CTA.
-template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
+template <typename T, int NT, int R, int JB, int TN, bool PIVOT, bool TC = false>
 __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* piv_out,
                                               int* info_out, int cw, bool fold,
                                               unsigned char* smem_raw)
@@ -218,6 +344,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
     static_assert(NT % 32 == 0 && NT <= 1024, "CTA size");
     using K = typename KeyOf<T>::type;
     using SM = CtaLuSmem<T, NT, JB>;
+    using Tile = typename TileOf<T, TC && JB % 8 == 0>::type;
     constexpr int NW = NT / 32;
     const int ldp = SM::ldp(m), cwp = SM::cwp(cw);
     T* sP = reinterpret_cast<T*>(smem_raw);          // [JB][ldp]
@@ -517,12 +644,12 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             __syncthreads();
             for(int t = warp; t < ncp / 32; t += NW)
             {
-                WarpTile<T> w;
+                Tile w;
                 w.zero();
                 int arow[4];
 #pragma unroll
                 for(int mi = 0; mi < 4; ++mi)
-                    arow[mi] = WarpTile<T>::frag_row(mi);
+                    arow[mi] = Tile::frag_row(mi);
                 w.template mma<JB>(sLi, SM::LDI, arow, sU, cwp, t * 32);
                 __syncwarp();
                 w.each([&](int rr, int cc, T& v) {
@@ -539,12 +666,12 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             for(int t = warp; t < tm * tn; t += NW)
             {
                 const int r0 = (t % tm) * 32, cc0 = (t / tm) * 32;
-                WarpTile<T> w;
+                Tile w;
                 int arow[4];
 #pragma unroll
                 for(int mi = 0; mi < 4; ++mi)
                 {
-                    const int r = r0 + WarpTile<T>::frag_row(mi);
+                    const int r = r0 + Tile::frag_row(mi);
                     arow[mi] = r < mt ? slotof[jb + r] : 0;
                 }
                 w.each([&](int rr, int cc, T& v) {
@@ -580,7 +707,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
 // 128-thread CTAs: 3 per SM, or LU_MIN_BLOCKS_128 when the panel fits the smaller register
 // budget (FP32, or one row per thread); 256-thread CTAs: LU_MIN_BLOCKS, or one per SM for
 // panels of more than 32 registers per thread (two rows of a 32-wide panel)
-template <typename T, int NT, int R, int JB, int TN, bool PIVOT>
+template <typename T, int NT, int R, int JB, int TN, bool PIVOT, bool TC = false>
 __global__ void __launch_bounds__(NT,
                                   NT <= 128 ? ((sizeof(T) == 4 || R == 1) ? LU_MIN_BLOCKS_128 : 3)
                                             : (R * JB > 32 ? 1 : LU_MIN_BLOCKS))
@@ -591,8 +718,9 @@ __global__ void __launch_bounds__(NT,
     const int64_t b = blockIdx.x;
     if(gate.skip(b))
         return;
-    getrf_cta_dev<T, NT, R, JB, TN, PIVOT>(m, n, A.at(b), lda, PIVOT ? ipiv + b * strideP : nullptr,
-                                           info + b, cw, fold != 0, smem_raw);
+    getrf_cta_dev<T, NT, R, JB, TN, PIVOT, TC>(m, n, A.at(b), lda,
+                                               PIVOT ? ipiv + b * strideP : nullptr, info + b,
+                                               cw, fold != 0, smem_raw);
 }
 
 } // namespace rsb

@@ -13,7 +13,8 @@
 //
 // Pipeline (all on the handle's stream, no host synchronisation):
 //   1. convert : A -> FP32 copy in the workspace, overflow flags, info = iter = 0
-//   2. sgetrf  : FP32 LU of the copy (same kernels as getrf, FP32 instantiation)
+//   2. sgetrf  : FP32 LU of the copy (the CTA LU kernels of getrf in FP32, with the trailing
+//                updates as split-TF32 tensor products: FP32-level accuracy)
 //   3. refine  : one CTA per matrix: x = LU32^{-1} b, then r = b - A x in FP64 (A read in
 //                FP64), d = LU32^{-1} r in FP32, x += d, until the stopping rule holds
 //   4. fallback: FP64 getrf + getrs gated to the members whose refinement failed.
@@ -681,7 +682,8 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
         if(cudaGetLastError() != cudaSuccess)
             return rocblas_status_internal_error;
         rocblas_status st = launch_getrf<float>(s, n, n, strided<float>(a32, (int64_t)n * n), n,
-                                                ipiv, strideP, info32, bc, true, Gate{flag, 0});
+                                                ipiv, strideP, info32, bc, true, Gate{flag, 0},
+                                                true);
         if(st != rocblas_status_success)
             return st;
         if(NRC == 1)

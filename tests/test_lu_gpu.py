@@ -121,6 +121,45 @@ def test_getrf_uniform_square(handle, n, dtype):
             assert be / (n * eps_of(dtype)) < 10
 
 
+@pytest.mark.parametrize("n", [16, 33, 64, 100, 128, 200, 256, 300, 512, 1024])
+def test_sgetrf_tf32(handle, n):
+    """rocsolver_sgetrf_tf32_strided_batched (split-TF32 tensor-core trailing updates, the
+    factorisation of dsgesv): info as the oracle's FP32 LU, FP32-level backward error
+    ||PA - LU||_F / (n ||A||_F eps32) < 10 with the returned pivots, and up to n = 512 the
+    oracle's pivots except where the different rounding flips a near tie (< 2 % of them;
+    at n = 1024 one early flip changes every later pivot, so only the backward error and
+    info are compared)."""
+    bc = 3
+    A = uniform_general(n, n, bc, seed=4000 + n).astype(np.float32)
+    dA = dev(to_colmajor(A))
+    dP = dev(np.full(bc * n, -7, np.int32))
+    dI = dev(np.full(bc, -7, np.int32))
+    st = rs.call("rocsolver_sgetrf_tf32_strided_batched", handle, n, n, ptr(dA), n, n * n,
+                 ptr(dP), n, ptr(dI), bc)
+    assert st == rs.SUCCESS, rs.STATUS_NAMES[st]
+    LU = from_colmajor(host(dA), bc, n, n, n, n * n)
+    ipiv, info = host(dP).reshape(bc, n), host(dI)
+    _, oipiv, oinfo = oracle_getrf(A)
+    np.testing.assert_array_equal(info, oinfo)
+    for b in range(bc):
+        be = lu_backward_error(A[b].astype(np.float64), LU[b].astype(np.float64), ipiv[b])
+        assert be / (n * eps_of(np.float32)) < 10, (b, be)
+    if n <= 512:
+        assert (ipiv != oipiv).mean() < 0.02
+
+
+def test_sgetrf_tf32_argument_checks(handle):
+    """Same checks and quick returns as sgetrf (roclapack_getrf_strided_batched.cpp:8-84)."""
+    dI = dev(np.full(2, -7, np.int32))
+    f = "rocsolver_sgetrf_tf32_strided_batched"
+    assert rs.call(f, None, 4, 4, None, 4, 16, None, 4, ptr(dI), 2) == rs.INVALID_HANDLE
+    assert rs.call(f, handle, -1, 4, None, 4, 16, None, 4, ptr(dI), 2) == rs.INVALID_SIZE
+    assert rs.call(f, handle, 4, 4, None, 3, 16, None, 4, ptr(dI), 2) == rs.INVALID_SIZE
+    assert rs.call(f, handle, 4, 4, None, 4, 16, None, 4, ptr(dI), 2) == rs.INVALID_POINTER
+    assert rs.call(f, handle, 0, 4, None, 1, 4, None, 4, ptr(dI), 2) == rs.SUCCESS
+    np.testing.assert_array_equal(host(dI), [0, 0])
+
+
 @pytest.mark.parametrize("m,n", [(1, 5), (5, 1), (7, 3), (3, 7), (31, 33), (33, 31), (64, 16),
                                  (16, 64), (200, 40), (40, 200), (513, 60), (192, 520),
                                  (640, 64), (1000, 45)])
