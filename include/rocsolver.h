@@ -845,9 +845,10 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_vbatched_noalloc(rocblas_handle 
 /* ---- Kernel configuration table (no counterpart in the reference, whose block sizes and
  * kernel switch points are compile-time constants: library/src/include/ideal_sizes.hpp:
  * 166-240, docs/design/tuning.rst:20-31).  The table is text, one entry per line:
- *   getrf    <s|d> <m_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold>
+ *   getrf    <s|d|t> <m_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold>
  *   vbatched <s|d> <n_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold> <ctas_per_sm>
- * It is written by the autotuner (python -m rocsolver_b200.tune) and read when the first
+ * (t: the FP32 LU with split-TF32 updates of sgetrf_tf32 and dsgesv; without t entries it
+ * uses the s entries).  It is written by the autotuner (python -m rocsolver_b200.tune) and read when the first
  * handle is created, from $ROCSOLVER_B200_TUNING or else tuning_b200.txt beside the
  * library.  Entries that name an unavailable configuration fall back to the built-in
  * choice; results do not depend on the table, only speed does. */

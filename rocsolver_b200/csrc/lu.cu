@@ -146,7 +146,8 @@ static rocblas_status getrf_dispatch(cudaStream_t s, int m, int n, Batch<T> A, i
         return launch_status();
     }
     LuCfg c;
-    if(tuned_getrf(sizeof(T) == 8 ? 'd' : 's', m, &c))
+    const char prec = sizeof(T) == 8 ? 'd' : 's';
+    if((TC && tuned_getrf('t', m, &c)) || tuned_getrf(prec, m, &c))
     {
         bool ran = false;
         const rocblas_status st =

@@ -69,7 +69,8 @@ bool parse(const char* text, Table* out)
         }
         else
             return false;
-        if(!(ls >> prec >> e.size_max) || (prec != "s" && prec != "d") || e.size_max < 1)
+        if(!(ls >> prec >> e.size_max) || e.size_max < 1
+           || !(prec == "s" || prec == "d" || (prec == "t" && e.kind == 0)))
             return false;
         e.prec = prec[0];
         for(int i = 0; i < nvals; ++i)

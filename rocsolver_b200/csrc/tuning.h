@@ -6,11 +6,12 @@
 // (docs/design/tuning.rst:20-31).  Here the choices live in a text table that the
 // autotuner measures on the GPU and the library reads when the first handle is created:
 //
-//   getrf    <s|d> <m_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold>
+//   getrf    <s|d|t> <m_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold>
 //   vbatched <s|d> <n_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold> <ctas_per_sm>
 //
 // An entry applies to sizes up to m_max (n_max: the batch's largest order) above the
-// previous entry of the same kind and precision.  chunk = trailing-update column chunk
+// previous entry of the same kind and precision (t = the FP32 LU with split-TF32 trailing
+// updates).  chunk = trailing-update column chunk
 // (multiple of 32; 0 = the default), fold = 1 folds each panel's row interchanges into the
 // trailing update, ctas_per_sm = resident CTAs the persistent kernel launches per SM
 // (0 = as many as fit).  Entries naming a kernel variant that is not compiled, or one too
@@ -30,7 +31,7 @@ struct VbCfg
     int nt, r, jb, cw, fold, per_sm;
 };
 
-// entry for (precision 's'/'d', size); false when the table has none
+// entry for (precision 's'/'d'/'t', size); false when the table has none
 bool tuned_getrf(char prec, int m, LuCfg* out);
 bool tuned_vbatched(char prec, int max_n, VbCfg* out);
 // load the table named by ROCSOLVER_B200_TUNING, else tuning_b200.txt beside the library

@@ -9,7 +9,8 @@ the class's largest size -- (threads, rows per thread, panel width), trailing-up
 column chunk, and whether the panel's row interchanges are folded into the trailing
 update -- on seeded uniform[-1, 1] batches, and keeps the fastest.  For the variable-size
 kernel it also tunes the number of resident CTAs per SM, on batches with n uniform in
-[8, n_max] and nrhs uniform in [1, 16].
+[8, n_max] and nrhs uniform in [1, 16].  Precision t is the FP32 LU with split-TF32
+trailing updates (rocsolver_sgetrf_tf32_strided_batched, the factorisation of dsgesv).
 
 The table (format in include/rocsolver.h, rocsolver_b200_tuning_set) is written to
 rocsolver_b200/tuning_b200.txt by default, where the library reads it when the first
@@ -74,7 +75,8 @@ def tune_getrf(prec, n, bc, reps, quick, log):
     ipiv = torch.zeros(bc * n, dtype=torch.int32, device="cuda")
     info = torch.zeros(bc, dtype=torch.int32, device="cuda")
     h = rs.Handle(torch.cuda.current_stream().cuda_stream)
-    fn_name = f"rocsolver_{prec}getrf_strided_batched"
+    fn_name = ("rocsolver_sgetrf_tf32_strided_batched" if prec == "t"
+               else f"rocsolver_{prec}getrf_strided_batched")
 
     def call():
         st = rs.call(fn_name, h.value, n, n, rs.ptr(A), n, n * n, rs.ptr(ipiv), n,
@@ -175,7 +177,7 @@ def main():
     ap.add_argument("--log", default=None, help="also append the measurements to this file")
     ap.add_argument("--classes", default=",".join(map(str, GETRF_CLASSES)))
     ap.add_argument("--vb-classes", default=",".join(map(str, VB_CLASSES)))
-    ap.add_argument("--precisions", default="d,s")
+    ap.add_argument("--precisions", default="d,s,t")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--quick", action="store_true", help="fewer chunk widths")
     a = ap.parse_args()
@@ -190,7 +192,7 @@ def main():
     old = rs.tuning_table()
     lines = [f"# written by python -m rocsolver_b200.tune on {torch.cuda.get_device_name()} "
              f"({datetime.date.today().isoformat()})",
-             "# getrf    <s|d> <m_max> <threads> <rows/thread> <panel> <chunk> <fold>"
+             "# getrf    <s|d|t> <m_max> <threads> <rows/thread> <panel> <chunk> <fold>"
              "    # ms: tuned / built-in",
              "# vbatched <s|d> <n_max> <threads> <rows/thread> <panel> <chunk> <fold> "
              "<ctas/SM>"]
@@ -201,7 +203,7 @@ def main():
                                          log)
                 lines.append(f"getrf {prec} {n} " + " ".join(map(str, cand))
                              + f"    # {t:.3f} / {tb:.3f} ms, batch {GETRF_CLASSES.get(n, 256)}")
-            for n in [int(x) for x in a.vb_classes.split(",") if x]:
+            for n in [int(x) for x in a.vb_classes.split(",") if x and prec != "t"]:
                 cand, t, tb = tune_vbatched(prec, n, VB_CLASSES.get(n, 1024), a.reps, a.quick,
                                             log)
                 lines.append(f"vbatched {prec} {n} " + " ".join(map(str, cand))

@@ -16,12 +16,14 @@ def test_roundtrip_sorted_and_comments():
                 "vbatched d 512 256 2 16 64 1 0\n"
                 "getrf d 256 256 1 32 64 0   # trailing comment\n"
                 "getrf d 128 128 1 32 0 1\n"
+                "getrf t 512 256 2 32 128 1\n"
                 "getrf s 256 128 2 32 96 1\n")
         assert rs.set_tuning_table(text) == SUCCESS
         got = rs.tuning_table().splitlines()
         assert got == ["getrf d 128 128 1 32 0 1",
                        "getrf d 256 256 1 32 64 0",
                        "getrf s 256 128 2 32 96 1",
+                       "getrf t 512 256 2 32 128 1",
                        "vbatched d 512 256 2 16 64 1 0"]
     finally:
         _restore(old)
@@ -34,7 +36,7 @@ def test_malformed_text_is_rejected_and_table_kept():
         for bad in ("getrf x 256 256 1 32 64 0", "getrf d 256 256 1 32 64",
                     "getrf d 256 256 1 32 64 0 9", "potrf d 64 1 2 3 4 5",
                     "getrf d 0 256 1 32 64 0", "getrf d 256 -1 1 32 64 0",
-                    "vbatched d 512 256 2 16 64 1"):
+                    "vbatched d 512 256 2 16 64 1", "vbatched t 512 256 2 16 64 1 0"):
             assert rs.set_tuning_table(bad) == INVALID_VALUE, bad
             assert rs.tuning_table() == "getrf d 256 256 1 32 64 0\n"
         assert rs.lib().rocsolver_b200_tuning_set(None) == INVALID_POINTER
