@@ -5,7 +5,9 @@
 
 Prints ONE JSON line on rank 0.  A "step" is one pass of the hot path over one batch of
 synthetic input already resident in HBM (value); "e2e" repeats it through the public C ABI
-with the inputs copied from pinned host memory and the solutions read back every step.
+with the inputs copied from pinned host memory and the solutions read back every step
+(batches of 64 MiB of inputs or more are streamed in 8 slices over 2 streams, so that
+copies overlap kernels).
 
 Workloads (synthetic inputs with the shapes and value distributions of the reference
 configurations; no dataset is involved):
@@ -410,9 +412,59 @@ def run_mixed(w, torch, rs, dev, handle, steps, warmup):
             "iter_max": int(its.max()), "fallbacks": int((its < 0).sum())}
 
 
+E2E_CHUNKS = 8    # batch slices per step in the end-to-end run (large inputs only)
+E2E_STREAMS = 2   # streams (one handle each) the slices alternate over
+E2E_MIN_BYTES = 64 << 20  # smaller steps are one slice: there the per-slice launches and
+                          # copies cost more than the overlap gains
+
+
+class SlicedStep:
+    """One end-to-end step as slices of the batch issued round-robin on E2E_STREAMS
+    streams, each with its own handle (and so its own workspace): body(handle, c0, c1)
+    copies members c0..c1-1 in, calls the library, copies the results out, all on the
+    current (slice) stream.  Steps with at least E2E_MIN_BYTES of copies are cut into
+    E2E_CHUNKS slices, so that one slice's copies overlap another slice's kernels and the
+    two copy directions overlap each other, as a caller streaming batches from the host
+    would; smaller steps are one slice.  step() spans the whole step: the slice streams
+    wait for an event on the main stream and the main stream waits for all of them."""
+
+    def __init__(self, torch, rs, bc, copy_bytes, body):
+        self.torch, self.body, self.bc = torch, body, bc
+        self.main = torch.cuda.current_stream()
+        chunks = E2E_CHUNKS if copy_bytes >= E2E_MIN_BYTES else 1
+        per = (bc + chunks - 1) // chunks
+        self.bounds = [(c0, min(bc, c0 + per)) for c0 in range(0, bc, per)]
+        self.streams = ([self.main] if len(self.bounds) == 1
+                        else [torch.cuda.Stream() for _ in range(E2E_STREAMS)])
+        self.handles = [rs.Handle(st.cuda_stream) for st in self.streams]
+        self.desc = (f"{len(self.bounds)} slices of <= {per} members over "
+                     f"{len(self.streams)} streams")
+
+    def step(self):
+        torch = self.torch
+        if len(self.bounds) == 1:  # one slice: the whole batch on the main stream
+            self.body(self.handles[0].value, 0, self.bc)
+            return
+        start = torch.cuda.Event()
+        start.record(self.main)
+        for i, (c0, c1) in enumerate(self.bounds):
+            st = self.streams[i % E2E_STREAMS]
+            st.wait_event(start)
+            with torch.cuda.stream(st):
+                self.body(self.handles[i % E2E_STREAMS].value, c0, c1)
+        for st in self.streams:
+            self.main.wait_stream(st)
+
+    def close(self):
+        self.torch.cuda.synchronize()
+        for h in self.handles:
+            h.close()
+
+
 def run_e2e(w, torch, rs, dev, handle, steps):
-    """Same step through the public C ABI with host buffers: pinned A and B copied H2D,
-    factor + solve, solutions and info copied D2H, every step."""
+    """Same step through the public C ABI with host buffers: every step copies the pinned
+    A and B to the device, factors and solves, and copies the solutions and info back
+    (streamed in slices, SlicedStep); all copies are inside the timed region."""
     n, bc, nrhs = w.n, w.bc, w.nrhs
     hA = w.A0.cpu().pin_memory()
     hB = w.B0.cpu().pin_memory()
@@ -420,48 +472,54 @@ def run_e2e(w, torch, rs, dev, handle, steps):
     hI = torch.empty(bc, dtype=torch.int32).pin_memory()
     dA = torch.empty_like(w.A0)
     dB = torch.empty_like(w.B0)
-    ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
-    info = torch.zeros(bc, dtype=torch.int32, device=dev)
-    stream = torch.cuda.current_stream()
-    h = handle.value
-
     dX = torch.empty_like(w.B0)
+    ipiv = torch.zeros(bc, n, dtype=torch.int32, device=dev)
+    info = torch.zeros(bc, dtype=torch.int32, device=dev)
     it = torch.zeros(bc, dtype=torch.int32, device=dev)
+    P = rs.ptr
+    h2d, d2h = hA.numel() * 8 + hB.numel() * 8, hX.numel() * 8 + bc * 4
 
-    def step():
-        dA.copy_(hA, non_blocking=True)
-        dB.copy_(hB, non_blocking=True)
+    def body(h, c0, c1):
+        m = c1 - c0
+        cut = (lambda t: t) if m == bc else (lambda t: t[c0:c1])
+        a, b, x = cut(dA), cut(dB), cut(dX)
+        pv, inf, itr = cut(ipiv), cut(info), cut(it)
+        a.copy_(cut(hA), non_blocking=True)
+        b.copy_(cut(hB), non_blocking=True)
         if w.name == "dsgesv_n256":
-            rs.check(rs.call("rocsolver_dsgesv_strided_batched", h, n, nrhs, rs.ptr(dA), n,
-                             n * n, rs.ptr(ipiv), n, rs.ptr(dB), n, n * nrhs, rs.ptr(dX), n,
-                             n * nrhs, rs.ptr(it), rs.ptr(info), bc), "dsgesv")
-            hX.copy_(dX, non_blocking=True)
-            hI.copy_(info, non_blocking=True)
-            return
-        if w.name == "potrf_n64":
+            rs.check(rs.call("rocsolver_dsgesv_strided_batched", h, n, nrhs, P(a), n, n * n,
+                             P(pv), n, P(b), n, n * nrhs, P(x), n, n * nrhs, P(itr), P(inf),
+                             m), "dsgesv")
+            out = x
+        elif w.name == "potrf_n64":
             rs.check(rs.call("rocsolver_dposv_strided_batched", h, rs.FILL_LOWER, n, nrhs,
-                             rs.ptr(dA), n, n * n, rs.ptr(dB), n, n * nrhs, rs.ptr(info), bc),
-                     "posv")
+                             P(a), n, n * n, P(b), n, n * nrhs, P(inf), m), "posv")
+            out = b
         else:
-            rs.check(rs.call("rocsolver_dgetrf_strided_batched", h, n, n, rs.ptr(dA), n, n * n,
-                             rs.ptr(ipiv), n, rs.ptr(info), bc), "getrf")
-            rs.check(rs.call("rocsolver_dgetrs_strided_batched", h, rs.OP_N, n, nrhs, rs.ptr(dA),
-                             n, n * n, rs.ptr(ipiv), n, rs.ptr(dB), n, n * nrhs, bc), "getrs")
-        hX.copy_(dB, non_blocking=True)
-        hI.copy_(info, non_blocking=True)
+            rs.check(rs.call("rocsolver_dgetrf_strided_batched", h, n, n, P(a), n, n * n,
+                             P(pv), n, P(inf), m), "getrf")
+            rs.check(rs.call("rocsolver_dgetrs_strided_batched", h, rs.OP_N, n, nrhs, P(a), n,
+                             n * n, P(pv), n, P(b), n, n * nrhs, m), "getrs")
+            out = b
+        cut(hX).copy_(out, non_blocking=True)
+        cut(hI).copy_(inf, non_blocking=True)
 
-    for _ in range(2):
-        step()
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    k = max(3, min(steps, 10))
-    a.record(stream)
-    for _ in range(k):
-        step()
-    b.record(stream)
-    torch.cuda.synchronize()
+    sl = SlicedStep(torch, rs, bc, h2d + d2h, body)
+    try:
+        for _ in range(2):
+            sl.step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k = max(3, min(steps, 10))
+        a.record(sl.main)
+        for _ in range(k):
+            sl.step()
+        b.record(sl.main)
+        torch.cuda.synchronize()
+    finally:
+        sl.close()
     ms = a.elapsed_time(b) / k
-    return {"ms": ms, "h2d": hA.numel() * 8 + hB.numel() * 8, "d2h": hX.numel() * 8 + bc * 4}
+    return {"ms": ms, "h2d": h2d, "d2h": d2h, "pipeline": sl.desc}
 
 
 # ----------------------------------------------------------------------------- CPU side
@@ -557,7 +615,8 @@ def main():
         "data": "synthetic (seeded, generated on device)", "config": w.config,
         "gpu_launches": w.launches_per_step * args.steps,
         "e2e": {"value": units / (e2e["ms"] / 1e3), "unit": w.unit,
-                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
+                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                "pipeline": e2e["pipeline"]},
         "roofline": {"bound": "hbm", "kernel": w.dominant, "achieved": achieved_gbs,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"],
@@ -855,6 +914,7 @@ def main_extra(args, rank, world, local):
             hX.copy_(B, non_blocking=True)
             hI.copy_(info, non_blocking=True)
         h2d, d2h = (hA.numel() + hB.numel()) * 8, hX.numel() * 8 + bc * 4
+        e2e_pipeline = "one graph replay of the whole batch on one stream"
     else:
         n, nrhs = w.n, w.nrhs
         call()
@@ -876,19 +936,26 @@ def main_extra(args, rank, world, local):
         dLU, dP = torch.empty_like(LU), torch.empty_like(ipiv)
         dX, dG = torch.empty_like(w.X0), torch.empty_like(w.G0)
 
-        def e2e_step():
-            dLU.copy_(hLU, non_blocking=True)
-            dP.copy_(hP, non_blocking=True)
-            dX.copy_(hX, non_blocking=True)
-            dG.copy_(hG, non_blocking=True)
-            rs.check(rs.call(f"rocsolver_{w.prec}getrs_adjoint_strided_batched", h, n, nrhs, P(dLU), n,
-                             n * n, P(dP), n, P(dX), n, n * nrhs, P(dG), n, n * nrhs, P(gA), n,
-                             n * n, P(gB), n, n * nrhs, bc), "adjoint")
-            hgA.copy_(gA, non_blocking=True)
-            hgB.copy_(gB, non_blocking=True)
         es = LU.element_size()
         h2d = (hLU.numel() + hX.numel() + hG.numel()) * es + hP.numel() * 4
         d2h = (hgA.numel() + hgB.numel()) * es
+
+        def body(hs, c0, c1):
+            sl_ = slice(c0, c1)
+            dLU[sl_].copy_(hLU[sl_], non_blocking=True)
+            dP.view(bc, n)[sl_].copy_(hP.view(bc, n)[sl_], non_blocking=True)
+            dX[sl_].copy_(hX[sl_], non_blocking=True)
+            dG[sl_].copy_(hG[sl_], non_blocking=True)
+            rs.check(rs.call(f"rocsolver_{w.prec}getrs_adjoint_strided_batched", hs, n, nrhs,
+                             P(dLU[sl_]), n, n * n, P(dP.view(bc, n)[sl_]), n, P(dX[sl_]), n,
+                             n * nrhs, P(dG[sl_]), n, n * nrhs, P(gA[sl_]), n, n * n,
+                             P(gB[sl_]), n, n * nrhs, c1 - c0), "adjoint")
+            hgA[sl_].copy_(gA[sl_], non_blocking=True)
+            hgB[sl_].copy_(gB[sl_], non_blocking=True)
+        sliced = SlicedStep(torch, rs, bc, h2d + d2h, body)
+        extra_handles += sliced.handles
+        e2e_step = sliced.step
+        e2e_pipeline = sliced.desc
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
@@ -908,7 +975,8 @@ def main_extra(args, rank, world, local):
             "data": "synthetic (seeded, generated on device)", "config": w.config,
             "gpu_launches": launches * args.steps,
             "e2e": {"value": bc * world / (e2e_ms / 1e3), "unit": w.unit,
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "pipeline": e2e_pipeline},
             "roofline": {"bound": "hbm", "kernel": "vb_persistent_kernel<double>"
                          if w.name == "vbatched_4096" else
                          f"solve_adjoint_kernel<{'float' if w.prec == 's' else 'double'}>",
