@@ -145,35 +145,12 @@ __device__ __forceinline__ int warp_argmax(uint32_t key, int row, bool valid, ui
 // otherwise divide (dgetf2; the reference always multiplies,
 // specialized/roclapack_getf2_specialized_kernels.hpp:96-99, which differs only for
 // subnormal pivots).  A zero pivot leaves the column unscaled.
+// (rcp: the correctly rounded reciprocal of piv, computed by the caller)
 template <typename T>
-struct Scaler
+__device__ __forceinline__ T getf2_scale(T x, T piv, T rcp)
 {
-    T piv, rcp;
-    int mode; // 0: zero pivot (no scaling), 1: multiply by rcp, 2: divide by piv
-    __device__ __forceinline__ void init(T p)
-    {
-        piv = p;
-        if(p == T(0))
-        {
-            mode = 0;
-            rcp = T(0);
-        }
-        else if(fabs(p) >= Lim<T>::sfmin())
-        {
-            mode = 1;
-            rcp = T(1) / p;
-        }
-        else
-        {
-            mode = 2;
-            rcp = T(0);
-        }
-    }
-    __device__ __forceinline__ T apply(T x) const
-    {
-        return mode == 1 ? x * rcp : (mode == 2 ? x / piv : x);
-    }
-};
+    return piv == T(0) ? x : (fabs(piv) >= Lim<T>::sfmin() ? x * rcp : x / piv);
+}
 
 // ---------------------------------------------------------------------------------------
 // Rolled register rows (LU panels): the active column is register 0 and a rank-1 update

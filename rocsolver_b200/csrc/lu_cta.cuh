@@ -66,6 +66,7 @@ struct CtaLuSmem
         s += sizeof(T) * 2 * NW;                // candidate pivot values
         s += sizeof(K) * 2 * NW;                // candidate keys
         s += sizeof(int) * 2 * NW;              // candidate positions
+        s += sizeof(int) * 2 * NW;              // candidate slots
         s += sizeof(int) * (size_t)R * NT;      // slot of each position
         s += sizeof(int) * 4 * JB;              // moved positions and their sources
         s += sizeof(int) * (JB + 2);            // panel pivots, counter
@@ -356,7 +357,8 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
     T* cpiv = crcp + 2 * NW;                           // [2][NW]
     K* ckey = reinterpret_cast<K*>(cpiv + 2 * NW);     // [2][NW]
     int* crow = reinterpret_cast<int*>(ckey + 2 * NW); // [2][NW]
-    int* slotof = crow + 2 * NW;                       // [R*NT]
+    int* cslot = crow + 2 * NW;                        // [2][NW]
+    int* slotof = cslot + 2 * NW;                      // [R*NT]
     int* moved = slotof + R * NT;                      // [2*JB]
     int* movsrc = moved + 2 * JB;                      // [2*JB]
     int* spiv = movsrc + 2 * JB;                       // [JB]
@@ -402,6 +404,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             {
                 K bk = 0;
                 int br = INT_MAX;
+                T bv = T(0);
                 bool any = false;
 #pragma unroll
                 for(int q = 0; q < R; ++q)
@@ -413,10 +416,14 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                         {
                             bk = kq;
                             br = lrow[q];
+                            bv = pv[q][0];
                             any = true;
                         }
                     }
                 }
+                // the candidate's reciprocal, formed while the reductions run (off the
+                // column's serial path)
+                const T brc = bv != T(0) ? Lim<T>::rcp(bv) : T(0);
                 K wk;
                 const int wr = warp_argmax(bk, br, any, &wk);
                 if(any && br == wr)
@@ -426,9 +433,9 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                         if(lrow[q] == wr && tid + q * NT < mp)
                         {
                             store_row_shifted<T, JB>(cb + warp * JB, pv[q]);
-                            const T p = pv[q][0];
-                            cpiv[buf * NW + warp] = p;
-                            crcp[buf * NW + warp] = p != T(0) ? Lim<T>::rcp(p) : T(0);
+                            cpiv[buf * NW + warp] = pv[q][0];
+                            crcp[buf * NW + warp] = brc;
+                            cslot[buf * NW + warp] = tid + q * NT;
                         }
                 }
                 if(lane == 0)
@@ -466,6 +473,11 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             const T* prowv = cb + gw * JB; // pivot row, shifted by one
             const T pivv = cpiv[buf * NW + gw];
             const T rcp = crcp[buf * NW + gw];
+            // row c of U: the pivot row's remaining panel entries, one per lane of the
+            // publishing warp (prowv holds columns c+1.. of the pivot row)
+            if(warp == gw && lane < jb - c)
+                sP[(c + lane) * ldp + (PIVOT ? cslot[buf * NW + gw] : c)] =
+                    lane == 0 ? pivv : prowv[lane - 1];
             if(tid == 0)
                 spiv[c] = prow;
             if(pivv == T(0) && inf == 0)
@@ -485,15 +497,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                 const int slot = tid + q * NT;
                 if(slot < mp)
                 {
-                    if(lrow[q] == c)
-                    {
-                        // the pivot row: its remaining panel entries are row c of U
-#pragma unroll
-                        for(int i = 0; i < JB; ++i)
-                            if(c + i < jb)
-                                sP[(c + i) * ldp + slot] = pv[q][i];
-                    }
-                    else if(lrow[q] > c)
+                    if(lrow[q] > c)
                     {
                         const T x = pv[q][0];
                         const T l = mode == 1 ? x * rcp : (mode == 2 ? x / pivv : x);

@@ -297,6 +297,8 @@ __device__ __forceinline__ void gesv_warp_dev(int n, int nrhs, T* a, int lda, in
         if(k < n)
         {
             const int buf = k & 1;
+            // every lane forms the reciprocal of its candidate while the reductions run
+            const T rck = r[k] != T(0) ? Lim<T>::rcp(r[k]) : T(0);
             typename KeyOf<T>::type kk;
             const int prow = warp_argmax(pivot_key(r[k], myrow == k), myrow,
                                          lane < n && myrow >= k, &kk);
@@ -306,6 +308,8 @@ __device__ __forceinline__ void gesv_warp_dev(int n, int nrhs, T* a, int lda, in
                 for(int j = k; j < NMAX; ++j)
                     srow[buf][j] = r[j];
             }
+            const int wl = __ffs(__ballot_sync(full, myrow == prow)) - 1;
+            const T rcp = __shfl_sync(full, rck, wl < 0 ? 0 : wl);
             __syncwarp();
             const T pivv = srow[buf][k];
             if(lane == k)
@@ -316,11 +320,9 @@ __device__ __forceinline__ void gesv_warp_dev(int n, int nrhs, T* a, int lda, in
                 myrow = k;
             else if(myrow == k)
                 myrow = prow;
-            Scaler<T> s;
-            s.init(pivv);
             if(lane < n && myrow > k)
             {
-                const T l = s.apply(r[k]);
+                const T l = getf2_scale(r[k], pivv, rcp);
                 r[k] = l;
 #pragma unroll
                 for(int j = k + 1; j < NMAX; ++j)
