@@ -40,6 +40,12 @@ constexpr int REFINE_BLOCKINV_MAXN = 512;
 #ifndef REFINE_NT
 #define REFINE_NT 256
 #endif
+// 8-column load batches in flight per residual row: 2 measured fastest on B200 at n = 256
+// (dsgesv step 4.10 ms; 1 batch 4.50 ms, 4 batches 4.39 ms with register spills)
+#ifndef REFINE_RES_UNROLL
+#define REFINE_RES_UNROLL 2
+#endif
+constexpr int kResUnroll = REFINE_RES_UNROLL;
 
 // A -> FP32 copy (ld n), FP32 overflow flag (LAPACK dsgesv: any |a_ij| > FLT_MAX sends
 // the member to the FP64 path), info = iter = 0.  One CTA per matrix, threads over rows,
@@ -262,17 +268,20 @@ __device__ void blockinv_sweep_pf(bool forward, const float* lu, int n, const fl
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nblk = (n + 31) / 32;
     const int i = tid;
-    float mv[32];
-    {
-        const int kb = forward ? 0 : (nblk - 1) * 32, nb = min(32, n - kb);
+    // this thread's row of the factor strip of sweep step bi (columns of block bi)
+    auto load_strip = [&](int bi, float (&v)[32]) {
+        const int blkid = forward ? bi : nblk - 1 - bi;
+        const int kb = blkid * 32, nb = min(32, n - kb);
         const bool act = forward ? (i >= kb + nb && i < n) : (i < kb);
         if(act)
         {
 #pragma unroll
             for(int k = 0; k < 32; ++k)
-                mv[k] = k < nb ? lu[i + (size_t)(kb + k) * n] : 0.f;
+                v[k] = k < nb ? lu[i + (size_t)(kb + k) * n] : 0.f;
         }
-    }
+    };
+    float mv[32];
+    load_strip(0, mv);
     for(int bi = 0; bi < nblk; ++bi)
     {
         const int blkid = forward ? bi : nblk - 1 - bi;
@@ -323,18 +332,10 @@ __device__ void blockinv_sweep_pf(bool forward, const float* lu, int n, const fl
                 if(c < nc)
                     s[i + c * n] = acc[c];
         }
-        // the next block's strip (its rows are a subset of this block's, or the same)
+        // the next step's strip (its rows are a subset of this step's, or the same); a
+        // second strip in flight does not fit the register budget of two CTAs per SM
         if(bi + 1 < nblk)
-        {
-            const int kb2 = forward ? kb + 32 : kb - 32, nb2 = min(32, n - kb2);
-            const bool act2 = forward ? (i >= kb2 + nb2 && i < n) : (i < kb2);
-            if(act2)
-            {
-#pragma unroll
-                for(int k = 0; k < 32; ++k)
-                    mv[k] = k < nb2 ? lu[i + (size_t)(kb2 + k) * n] : 0.f;
-            }
-        }
+            load_strip(bi + 1, mv);
         __syncthreads();
     }
 }
@@ -356,7 +357,7 @@ __device__ double residual_rows(const double* a, int lda, const double* bb, int 
             acc[c] = c < nc ? bb[ix(i, c0 + c, ldb)] : 0.0;
         double asum = 0.0;
         int j = 0;
-#pragma unroll 2
+#pragma unroll kResUnroll
         for(; j + 8 <= n; j += 8)
         {
             double v[8];
