@@ -194,8 +194,8 @@ def build_workload(name, torch, rs, dev, handle):
         w.bytes_per_unit_getrf = 2 * n * n * 8 + 4 * n + 4
         w.dominant = "getrf_cta_kernel<double, 256, 1, 32>"
         # DRAM bytes per member of the dominant kernel, from one ncu capture at batch 512
-        # (profiles/getrf_cta_fp64_n256_b512.md: 1443.0 MB / 512)
-        w.traffic_per_unit = 1443046400 / 512
+        # (profiles/getrf_cta_fp64_n256_b512.md: 1432.9 MB / 512)
+        w.traffic_per_unit = 1432930560 / 512
         w.launches_per_step = 2
         if name == "dsgesv_n256":
             w.metric = ("batched solves/s at FP64 backward err <=1e-13: mixed+IR vs plain FP64 LU")
@@ -204,8 +204,8 @@ def build_workload(name, torch, rs, dev, handle):
                                     "cond log-uniform [1e1,1e6]")
             w.dominant = ("getrf_cta_kernel<float, 128, 2, 32, TF32> (FP32 LU with split-TF32 "
                           "tensor-core trailing updates inside dsgesv)")
-            # profiles/getrf_cta_tf32_n256_b512.md: 712.4 MB / 512
-            w.traffic_per_unit = 712355840 / 512
+            # profiles/getrf_cta_tf32_n256_b512.md: 714.1 MB / 512
+            w.traffic_per_unit = 714073856 / 512
             w.launches_per_step = 6
     elif name == "getrf_n32":
         n, bc, nrhs = 32, 1000, 1
