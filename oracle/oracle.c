@@ -292,7 +292,8 @@ DEFINE_ORACLE(s, float, FLT_MIN, sqrtf)
 /* ---------------------------------------------------------------------- */
 /* Batch drivers: member b of a strided batch starts at X + b*strideX.  The
  * batch is split statically over nthreads pthreads (one LAPACK-style call per
- * member, as BASELINE's CPU arm and testing_getf2_getrf.hpp:290-296 do). */
+ * member, as the reference's host-LAPACK test path, testing_getf2_getrf.hpp:290-296,
+ * does). */
 typedef struct
 {
     int op; /* 0 getrf, 1 getrs, 2 potrf, 3 potrs, 4 gesv, 5 posv */
