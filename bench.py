@@ -48,17 +48,26 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 
+WORKLOADS = ("dsgesv_n256", "gesv_n256", "getrf_n32", "potrf_n64", "vbatched_4096",
+             "adjoint_n128", "adjoint_n128_fp32")
+EXTRA_WORKLOADS = ("vbatched_4096", "adjoint_n128", "adjoint_n128_fp32")
+# the workloads measured beside the headline in the default run (C1, C2, C4, C5)
+NESTED = ("getrf_n32", "potrf_n64", "vbatched_4096", "adjoint_n128", "adjoint_n128_fp32")
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="dsgesv_n256",
-                   choices=["dsgesv_n256", "gesv_n256", "getrf_n32", "potrf_n64",
-                            "vbatched_4096", "adjoint_n128", "adjoint_n128_fp32"])
+    p.add_argument("--workload", default="all", choices=["all"] + list(WORKLOADS),
+                   help="all (default): the dsgesv_n256 headline line, with every other "
+                        "workload measured in the same run under its \"configs\" key")
     p.add_argument("--cpu-seconds", type=float, default=12.0,
-                   help="target CPU time of the bounded CPU-baseline sample")
+                   help="target CPU time of the bounded CPU-baseline sample (all cores)")
+    p.add_argument("--cpu-seconds-extra", type=float, default=3.0,
+                   help="the same for each workload nested under \"configs\"")
     return p.parse_args()
 
 
@@ -193,9 +202,11 @@ def build_workload(name, torch, rs, dev, handle):
         w.flops_per_unit = 2.0 * n ** 3 / 3 + 2.0 * n * n * nrhs
         w.bytes_per_unit_getrf = 2 * n * n * 8 + 4 * n + 4
         w.dominant = "getrf_cta_kernel<double, 256, 1, 32>"
-        # DRAM bytes per member of the dominant kernel, from one ncu capture at batch 512
-        # (profiles/getrf_cta_fp64_n256_b512.md: 1432.9 MB / 512)
+        # DRAM bytes (read + write) per member of the dominant kernel: 1432.9 MB per 512
+        # members from `ncu --set full --clock-control none -c 1 -k regex:getrf_cta
+        # python -m rocsolver_b200.demo --case getrf --n 256 --batch 512 --reps 2`
         w.traffic_per_unit = 1432930560 / 512
+        w.limiter = "latency: the per-column pivot chain (FP64 compute fraction beside it)"
         w.launches_per_step = 2
         if name == "dsgesv_n256":
             w.metric = ("batched solves/s at FP64 backward err <=1e-13: mixed+IR vs plain FP64 LU")
@@ -204,8 +215,11 @@ def build_workload(name, torch, rs, dev, handle):
                                     "cond log-uniform [1e1,1e6]")
             w.dominant = ("getrf_cta_kernel<float, 128, 2, 32, TF32> (FP32 LU with split-TF32 "
                           "tensor-core trailing updates inside dsgesv)")
-            # profiles/getrf_cta_tf32_n256_b512.md: 714.1 MB / 512
+            # 714.1 MB per 512 members from `ncu --set full --clock-control none -c 1
+            # -k regex:getrf_cta python -m rocsolver_b200.demo --case dsgesv --n 256
+            # --batch 512 --reps 1`
             w.traffic_per_unit = 714073856 / 512
+            w.limiter = "latency: the per-column pivot chain (TF32 tensor fraction beside it)"
             w.launches_per_step = 6
     elif name == "getrf_n32":
         n, bc, nrhs = 32, 1000, 1
@@ -226,10 +240,12 @@ def build_workload(name, torch, rs, dev, handle):
         w.flops_per_unit = 2.0 * n ** 3 / 3 + 2.0 * n * n * nrhs
         w.bytes_per_unit_getrf = 2 * n * n * 8 + 4 * n + 4
         w.dominant = "getrf_warp_kernel<double, 32>"
-        # profiles/getrf_warp_fp64_n32_b1000.md captures one 8 MB batch, which stays in L2
-        # under replay (8.3 MB / 1000); the bench rotates 24 copies so its traffic is the
-        # algorithmic figure
+        # one ncu capture of the 8 MB batch (`ncu --set full --clock-control none -c 1
+        # -k regex:getrf_warp python -m rocsolver_b200.demo --case getrf --n 32 --batch 1000
+        # --reps 2`) reads 8.3 MB per 1000 members; the bench rotates 24 copies so that its
+        # traffic is the algorithmic figure
         w.traffic_per_unit = 8269824 / 1000
+        w.limiter = "latency: one serial 32-column chain per matrix"
         w.launches_per_step = 2
     elif name == "potrf_n64":
         n, bc, nrhs = 64, 20000, 4
@@ -252,8 +268,11 @@ def build_workload(name, torch, rs, dev, handle):
         w.flops_per_unit = n ** 3 / 3.0 + n * n / 2.0 + n / 6.0 + 2.0 * n * n * nrhs
         w.bytes_per_unit_getrf = 2 * (n * (n + 1) // 2) * 8 + 4  # triangle read+write + info
         w.dominant = "potrf_reg_kernel<double, 64>"
-        # profiles/potrf_reg_fp64_n64_b4000.md: 105.6 MB / 4000
+        # 105.6 MB per 4000 members from `ncu --set full --clock-control none -c 1
+        # -k regex:potrf_reg python -m rocsolver_b200.demo --case potrf --n 64 --batch 4000
+        # --reps 2`
         w.traffic_per_unit = 105635840 / 4000
+        w.limiter = "latency: one barrier per column"
         w.launches_per_step = 2
     else:
         raise ValueError(name)
@@ -523,49 +542,147 @@ def run_e2e(w, torch, rs, dev, handle, steps):
 
 
 # ----------------------------------------------------------------------------- CPU side
-def cpu_sample(w, target_s):
-    """Time the oracle (unblocked LAPACK-algorithm restatement, one call per member,
-    members split over all host threads) on a bounded sample of the same inputs."""
-    import oracle
-    n, nrhs = w.n, w.nrhs
-    Ah = w.A0.cpu().numpy()
-    Bh = w.B0.cpu().numpy()
-    threads = oracle.nthreads_default()
+def _host_inputs(w):
+    """Host copies of the workload's inputs (column-major members, flat buffers)."""
+    if not hasattr(w, "host"):
+        if w.name == "vbatched_4096":
+            w.host = (w.sizes.cpu().numpy().astype(np.int32), w.rhs.cpu().numpy().astype(np.int32),
+                      w.A0.cpu().numpy(), w.B0.cpu().numpy())
+        elif w.name.startswith("adjoint"):
+            w.host = (w.A0.double().cpu().numpy(), w.X0.double().cpu().numpy(),
+                      w.G0.double().cpu().numpy())
+        else:
+            w.host = (w.A0.cpu().numpy(), w.B0.cpu().numpy())
+    return w.host
 
-    def run(cnt):
-        cnt = min(cnt, w.bc)
-        A = Ah[:cnt].reshape(-1).copy()
-        B = Bh[:cnt].reshape(-1).copy()
-        ipiv = np.zeros(cnt * n, np.int32)
+
+def _lapack_run(w, routine, cnt, threads):
+    """One host-LAPACK pass over the first cnt members; returns seconds."""
+    import oracle
+    cnt = min(cnt, w.bc)
+    if w.name == "vbatched_4096":
+        sz, kk, A0, B0 = _host_inputs(w)
+        nmax = w.nmax
+        A = A0[:cnt].reshape(-1).copy()
+        B = B0[:cnt].reshape(-1).copy()
+        ipiv = np.zeros(cnt * nmax, np.int32)
         info = np.zeros(cnt, np.int32)
         t0 = time.perf_counter()
-        if w.name == "potrf_n64":
-            oracle.posv(False, n, nrhs, A, n, n * n, B, n, n * nrhs, info, cnt, nthreads=threads)
-        else:
-            oracle.getrf(n, n, A, n, n * n, ipiv, n, info, cnt, nthreads=threads)
-            oracle.getrs(0, n, nrhs, A, n, n * n, ipiv, n, B, n, n * nrhs, cnt, nthreads=threads)
-        return time.perf_counter() - t0, cnt
+        oracle.lapack_batch(oracle.LH_VGESV, nmax, 16, A, nmax, nmax * nmax, ipiv, nmax, B, nmax,
+                            16 * nmax, info=info, nv=sz, rv=kk, ld=nmax, bc=cnt, nthreads=threads)
+        return time.perf_counter() - t0
+    if w.name.startswith("adjoint"):
+        A0, X0, G0 = _host_inputs(w)
+        n, k = w.n, w.nrhs
+        if not hasattr(w, "host_lu"):  # factored once, outside the timing, like the GPU arm
+            LU = A0.reshape(-1).copy()
+            piv = np.zeros(w.bc * n, np.int32)
+            inf = np.zeros(w.bc, np.int32)
+            oracle.lapack_batch(oracle.LH_GETRF_GETRS, n, 0, LU, n, n * n, piv, n, None, n, 0,
+                                info=inf, bc=w.bc, nthreads=oracle.physical_cores())
+            w.host_lu = (LU, piv)
+        LU, piv = w.host_lu
+        gB = G0[:cnt].reshape(-1).copy()
+        gA = np.empty(cnt * n * n)
+        t0 = time.perf_counter()
+        oracle.lapack_batch(oracle.LH_ADJOINT, n, k, LU, n, n * n, piv, n, gB, n, n * k,
+                            bc=cnt, nthreads=threads)
+        oracle.lapack_outer(n, k, gB, X0[:cnt].reshape(-1), gA, cnt, nthreads=threads)
+        return time.perf_counter() - t0
+    A0, B0 = _host_inputs(w)
+    n, k = w.n, w.nrhs
+    A = A0[:cnt].reshape(-1).copy()
+    B = B0[:cnt].reshape(-1).copy()
+    ipiv = np.zeros(cnt * n, np.int32)
+    info = np.zeros(cnt, np.int32)
+    X = np.zeros_like(B) if routine == "dsgesv" else None
+    it = np.zeros(cnt, np.int32) if routine == "dsgesv" else None
+    op = {"getrf+getrs": oracle.LH_GETRF_GETRS, "potrf+potrs": oracle.LH_POTRF_POTRS,
+          "gesv": oracle.LH_GESV, "dsgesv": oracle.LH_DSGESV}[routine]
+    t0 = time.perf_counter()
+    oracle.lapack_batch(op, n, k, A, n, n * n, ipiv, n, B, n, n * k, X, n, n * k, info, it,
+                        bc=cnt, nthreads=threads)
+    return time.perf_counter() - t0
 
-    t, c = run(max(threads, 8))
-    want = int(c * max(1.0, target_s / max(t, 1e-6)))
-    want = max(c, min(want, w.bc))
-    t, c = run(want)
-    reps = 1
-    # a whole batch faster than the target: repeat it (fresh copies of the same inputs)
-    if c == w.bc and t < target_s:
+
+def _lapack_rate(w, routine, threads, target_s):
+    """Members per second of one routine on a bounded sample: a calibration pass, then
+    enough members (repeating the whole batch if needed) to take about target_s."""
+    c = max(threads * 2, 8)
+    t = _lapack_run(w, routine, c, threads)
+    c = min(c, w.bc)
+    want = max(c, min(w.bc, int(c * max(1.0, target_s / max(t, 1e-6)))))
+    t = _lapack_run(w, routine, want, threads)
+    reps, tot = 1, t
+    if want == w.bc and t < target_s:
         reps = max(1, int(target_s / max(t, 1e-6)))
-        tt = 0.0
-        for _ in range(reps):
-            tt += run(c)[0]
-        t = tt
-    return {"value": reps * c / t, "unit": w.unit, "cores": threads, "kind": "port",
-            "sample": f"{c} of {w.bc} members of the same batch"
-                      + (f", {reps} times" if reps > 1 else "")
-                      + f", oracle/oracle.c (unblocked LAPACK getf2/getrs or potf2/potrs "
-                      f"restatement), {threads} pthreads, {t:.1f} s"}
+        tot = sum(_lapack_run(w, routine, want, threads) for _ in range(reps))
+    return reps * want / tot, f"{want} of {w.bc} members" + (f" x {reps}" if reps > 1 else "") \
+        + f" in {tot:.1f} s"
+
+
+def _lapack_routines(w):
+    """Host-LAPACK routines timed for a workload (the reference's CPU path for it)."""
+    return {"dsgesv_n256": ["dsgesv", "gesv"], "gesv_n256": ["gesv"],
+            "getrf_n32": ["getrf+getrs"], "potrf_n64": ["potrf+potrs"],
+            "vbatched_4096": ["gesv (per-member n, nrhs)"],
+            "adjoint_n128": ["getrs (trans T) + dgemm"],
+            "adjoint_n128_fp32": ["getrs (trans T) + dgemm"]}[w.name]
+
+
+def cpu_sample(w, target_s, one_core_s=None):
+    """Host LAPACK (scipy's bundled OpenBLAS, loaded with dlopen; one call per member on one
+    thread, the batch split statically over all physical cores) on a bounded sample of the
+    same inputs, plus the 1-core figure (the reference client's serial loop).  For the
+    mixed-precision headline both LAPACK dsgesv (the CPU analogue of the mixed path) and
+    dgesv are timed and the faster is the value."""
+    import oracle
+    if not oracle.lapack_available():
+        raise RuntimeError("host LAPACK (scipy's OpenBLAS) is not available on this host")
+    cores = oracle.physical_cores()
+    one_core_s = target_s / 4 if one_core_s is None else one_core_s
+    routines = _lapack_routines(w)
+    per = {}
+    for r in routines:
+        key = r.split(" ")[0]
+        v, samp = _lapack_rate(w, key, cores, target_s / len(routines))
+        v1, samp1 = _lapack_rate(w, key, 1, one_core_s / len(routines))
+        per[r] = {"value": v, "sample": samp, "one_core": v1, "one_core_sample": samp1}
+    best = max(per, key=lambda r: per[r]["value"])
+    return {"value": per[best]["value"], "unit": w.unit, "cores": cores, "kind": "lapack",
+            "routine": best, "one_core": per[best]["one_core"],
+            "library": f"OpenBLAS bundled with scipy ({oracle.lapack_library_name()}), dlopen",
+            "cpu_model": oracle.cpu_model(), "nproc": os.cpu_count(),
+            "sample": f"host LAPACK {best}: {per[best]['sample']}, {cores} threads "
+                      f"(one member per call); 1 core: {per[best]['one_core_sample']}",
+            "routines": per}
 
 
 # ----------------------------------------------------------------------------- main
+class Ctx:
+    """What every workload runner shares: torch, the library, the device, the process group
+    (None on one GPU), the handle on the current stream, and this process's rank."""
+    pass
+
+
+def fp64_peak_tflops(torch, dev):
+    """FP64 dense peak measured in this run: cuBLAS dgemm 8192^3 (torch.matmul), best of 3
+    CUDA-event timings.  Only the denominator of the FP64 compute fraction."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    best = None
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    return 2.0 * 8192 ** 3 / (best / 1e3) / 1e12
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -574,65 +691,106 @@ def main():
 
     if args.impl == "reference":
         return main_reference(args, rank, world)
-    if args.workload in ("vbatched_4096", "adjoint_n128", "adjoint_n128_fp32"):
-        return main_extra(args, rank, world, local)
 
     import torch
     import rocsolver_b200 as rs
     torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    pg = None
+    ctx = Ctx()
+    ctx.torch, ctx.rs = torch, rs
+    ctx.dev = torch.device("cuda", local)
+    ctx.rank, ctx.world, ctx.local = rank, world, local
+    ctx.pg = None
     if world > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
-    handle = rs.Handle(torch.cuda.current_stream().cuda_stream)
-    w = build_workload(args.workload, torch, rs, dev, handle)
+        ctx.pg = dist
+    ctx.handle = rs.Handle(torch.cuda.current_stream().cuda_stream)
+    ctx.peaks = load_peaks()
+    ctx.peaks["fp64_tflops"] = fp64_peak_tflops(torch, ctx.dev)
+    headline = "dsgesv_n256" if args.workload == "all" else args.workload
+    line = run_workload(headline, args, ctx, args.steps, args.warmup, args.cpu_seconds)
+    if args.workload == "all":
+        # the other configurations, measured in the same run (fewer steps; same contract)
+        nested = {}
+        for name in NESTED:
+            sub = run_workload(name, args, ctx, min(args.steps, 10), max(3, min(args.warmup, 3)),
+                               args.cpu_seconds_extra)
+            for k in ("n_gpus", "higher_is_better", "scaling", "vs_baseline", "data"):
+                sub.pop(k, None)
+            nested[name] = sub
+            torch.cuda.empty_cache()
+        line["configs"] = nested
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.handle.close()
+    if ctx.pg:
+        ctx.pg.barrier()
+        ctx.pg.destroy_process_group()
+
+
+def run_workload(name, args, ctx, steps, warmup, cpu_seconds):
+    if name in EXTRA_WORKLOADS:
+        return run_extra(name, args, ctx, steps, warmup, cpu_seconds)
+    return run_core(name, args, ctx, steps, warmup, cpu_seconds)
+
+
+def run_core(name, args, ctx, steps, warmup, cpu_seconds):
+    """The strided-batched workloads (C1, C2, C3): one JSON line as a dict."""
+    torch, rs, dev, pg, handle = ctx.torch, ctx.rs, ctx.dev, ctx.pg, ctx.handle
+    world, rank = ctx.world, ctx.rank
+    w = build_workload(name, torch, rs, dev, handle)
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
     plain = None
     if w.name == "dsgesv_n256":
-        plain = run_ours(w, torch, rs, dev, handle, args.steps, args.warmup)
-        res = run_mixed(w, torch, rs, dev, handle, args.steps, args.warmup)
+        plain = run_ours(w, torch, rs, dev, handle, steps, warmup)
+        res = run_mixed(w, torch, rs, dev, handle, steps, warmup)
     else:
-        res = run_ours(w, torch, rs, dev, handle, args.steps, args.warmup)
+        res = run_ours(w, torch, rs, dev, handle, steps, warmup)
     total_ms = sum(res["step_ms"])
     total_ms = max_over_ranks(torch, pg, total_ms, dev)
-    e2e = run_e2e(w, torch, rs, dev, handle, args.steps)
+    e2e = run_e2e(w, torch, rs, dev, handle, steps)
     e2e["ms"] = max_over_ranks(torch, pg, e2e["ms"], dev)
-    ms_per_step = total_ms / args.steps
+    ms_per_step = total_ms / steps
     units = w.bc * world
     value = units / (ms_per_step / 1e3)
-    peaks = load_peaks()
+    peaks = ctx.peaks
     fact_s = res["fact_ms"] / 1e3
     achieved_gbs = w.bytes_per_unit_getrf * w.bc / fact_s / 1e9
+    fp64_tf = w.flops_per_unit * w.bc / fact_s / 1e12
     line = {
         "metric": w.metric, "value": value, "unit": w.unit, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "steps": steps, "warmup": warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
         "data": "synthetic (seeded, generated on device)", "config": w.config,
-        "gpu_launches": w.launches_per_step * args.steps,
+        "gpu_launches": w.launches_per_step * steps,
         "e2e": {"value": units / (e2e["ms"] / 1e3), "unit": w.unit,
                 "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
                 "pipeline": e2e["pipeline"]},
-        "roofline": {"bound": "hbm", "kernel": w.dominant, "achieved": achieved_gbs,
+        "roofline": {"bound": "hbm", "limiter": w.limiter, "kernel": w.dominant, "achieved": achieved_gbs,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"],
                      "traffic": w.traffic_per_unit * w.bc,
                      "peak_source": peaks["source"],
                      "kernel_ms": res["fact_ms"],
-                     "fp64_tflops": w.flops_per_unit * w.bc / fact_s / 1e12},
+                     "compute": {"achieved_tflops": fp64_tf, "peak_tflops": peaks["fp64_tflops"],
+                                 "frac": fp64_tf / peaks["fp64_tflops"],
+                                 "peak": "FP64 dgemm measured in this run (cuBLAS 8192^3)"}},
         "clocks": res["clocks"],
         "accuracy": {"backward_err_max": res["berr_max"],
                      "frac_backward_err_le_1e-13": res["berr_frac_1e13"],
                      "info_nonzero": res["info_nonzero"]},
     }
     if plain is not None:
-        plain_ms = sum(plain["step_ms"]) / args.steps
+        plain_ms = sum(plain["step_ms"]) / steps
+        plain_ms = max_over_ranks(torch, pg, plain_ms, dev)
+        pf_tf = w.flops_per_unit * w.bc / (plain["fact_ms"] / 1e3) / 1e12
         line["plain_fp64"] = {"value": units / (plain_ms / 1e3), "unit": w.unit,
                               "ms_per_step": plain_ms, "getrf_ms": plain["fact_ms"],
+                              "getrf_fp64_tflops": pf_tf,
+                              "getrf_fp64_frac": pf_tf / peaks["fp64_tflops"],
                               "backward_err_max": plain["berr_max"],
                               "frac_backward_err_le_1e-13": plain["berr_frac_1e13"]}
         line["mixed_over_plain"] = plain_ms / ms_per_step
@@ -640,48 +798,54 @@ def main():
                                  "fp64_fallbacks": res["fallbacks"]})
         fbytes = (2 * w.n * w.n * 4 + 4 * w.n + 4) * w.bc
         fgbs = fbytes / (res["fact_ms"] / 1e3) / 1e9
-        line["roofline"] = {"bound": "hbm", "kernel": w.dominant, "achieved": fgbs,
+        tf = w.flops_per_unit * w.bc / (res["fact_ms"] / 1e3) / 1e12
+        tf32_peak = peaks["bf16_tflops"] / 2
+        line["roofline"] = {"bound": "hbm", "limiter": w.limiter, "kernel": w.dominant, "achieved": fgbs,
                             "peak": peaks["hbm_gbs"], "unit": "GB/s",
                             "frac": fgbs / peaks["hbm_gbs"],
                             "traffic": w.traffic_per_unit * w.bc,
                             "peak_source": peaks["source"], "kernel_ms": res["fact_ms"],
-                            "fp32_tflops": w.flops_per_unit * w.bc / (res["fact_ms"] / 1e3)
-                            / 1e12}
+                            "compute": {"achieved_tflops": tf, "peak_tflops": tf32_peak,
+                                        "frac": 3 * tf / tf32_peak,
+                                        "peak": "dense TF32 tensor rate = half the measured "
+                                                "bf16 figure; frac counts the 3 split-TF32 "
+                                                "products per FP32 multiply-add"}}
+        if "stages_ms" in res:
+            line["mixed_stages_ms"] = res["stages_ms"]
     if rank == 0 and world == 1:
-        line["cpu_baseline"] = cpu_sample(w, args.cpu_seconds)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    handle.close()
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+        line["cpu_baseline"] = cpu_sample(w, cpu_seconds)
+    del w
+    return line
 
 
 def main_reference(args, rank, world):
     """Reference arm: the reference's own path is HIP/rocBLAS for AMD GPUs and cannot run
-    here; its CPU implementation of the path is host LAPACK, restated by the oracle.  Rank 0
-    times the oracle on the host cores over a bounded sample of the same workload."""
+    here; its CPU implementation of the path is host LAPACK (its clients' oracle and CPU
+    timing).  Rank 0 times host LAPACK (scipy's OpenBLAS, dlopen) on all physical host cores
+    over a bounded sample of the same workload; the other ranks exit without work."""
     if rank != 0:
         return
     import torch
     dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
-    extra = args.workload in ("vbatched_4096", "adjoint_n128", "adjoint_n128_fp32")
-    w = (_extra_workload(args.workload, torch, dev) if extra
-         else build_workload(args.workload, torch, None, dev, None))
+    name = "dsgesv_n256" if args.workload == "all" else args.workload
+    w = (_extra_workload(name, torch, dev) if name in EXTRA_WORKLOADS
+         else build_workload(name, torch, None, dev, None))
     w.dtype = getattr(w, "dtype", "f64")
     vals = []
+    r = None
     for i in range(args.warmup + args.steps):
-        sample = cpu_sample_extra if extra else cpu_sample
-        r = sample(w, max(1.0, args.cpu_seconds / max(1, args.steps)))
+        r = cpu_sample(w, max(1.0, args.cpu_seconds / max(1, args.steps)),
+                       one_core_s=0.5 if i < args.warmup + args.steps - 1 else 2.0)
         if i >= args.warmup:
             vals.append(r["value"])
     v = statistics.median(vals)
+    cb = dict(r)
+    cb["value"] = v
     line = {"metric": w.metric, "value": v, "unit": w.unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * w.bc / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
             "data": "synthetic (seeded)", "config": w.config, "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": w.unit, "cores": r["cores"], "kind": "port",
-                             "sample": r["sample"]},
+            "cpu_baseline": cb,
             "e2e": {"value": v, "unit": w.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -717,8 +881,9 @@ def _extra_workload(name, torch, dev):
         k = w.rhs.double()
         w.bytes_total = float((2 * n * n * 8 + 2 * n * k * 8 + 4 * n + 4).sum())
         w.flops_total = float((2 * n ** 3 / 3 + 2 * n * n * k).sum())
-        # DRAM bytes per member from one ncu capture of 512 members of the same
-        # distribution (profiles/vb_persistent_fp64_nmax512_b512.md: 4464.1 MB / 512)
+        # DRAM bytes per member: 4464.1 MB per 512 members of the same distribution from
+        # `ncu --set full --clock-control none -c 1 -k regex:vb_persistent python -m
+        # rocsolver_b200.demo --case vbatched --n 512 --batch 512 --nrhs 16 --reps 2`
         w.traffic_per_unit = 4464067000 / 512
     else:
         w.bc, w.n, w.nrhs = 8192, 128, 8
@@ -744,30 +909,22 @@ def _extra_workload(name, torch, dev):
                     "l2": f"factors {bc * n * n * es / 2**30:.1f} GiB > L2"}
         w.bytes_total = bc * (2 * n * n * es + 4 * n * nrhs * es + 4 * n)
         w.flops_total = bc * (4.0 * n * n * nrhs)
-        # profiles/solve_adjoint_fp64_n128_b1024.md: 245.5 MB / 1024 (FP64; FP32 scaled by
-        # the element size)
+        # 245.5 MB per 1024 FP64 members from `ncu --set full --clock-control none -c 1
+        # -k regex:solve_adjoint python -m rocsolver_b200.demo --case adjoint --n 128
+        # --batch 1024 --nrhs 8 --reps 2` (FP32 scaled by the element size)
         w.traffic_per_unit = 245479424 / 1024 * es / 8
     return w
 
 
-def main_extra(args, rank, world, local):
-    """The variable-size and adjoint rows: same contract as main() (one JSON line on rank
-    0, device time = max over ranks, e2e through the C ABI with host buffers)."""
-    import torch
-    import rocsolver_b200 as rs
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
-    handle = rs.Handle(torch.cuda.current_stream().cuda_stream)
+def run_extra(name, args, ctx, steps, warmup, cpu_seconds):
+    """The variable-size and adjoint rows (C4, C5): same contract as run_core (one JSON line
+    as a dict, device time = max over ranks, e2e through the C ABI with host buffers)."""
+    torch, rs, dev, pg, handle = ctx.torch, ctx.rs, ctx.dev, ctx.pg, ctx.handle
+    world, rank = ctx.world, ctx.rank
     h = handle.value
     extra_handles = []
     graph = None
-    w = _extra_workload(args.workload, torch, dev)
+    w = _extra_workload(name, torch, dev)
     stream = torch.cuda.current_stream()
     P = rs.ptr
     bc = w.bc
@@ -828,18 +985,18 @@ def main_extra(args, rank, world, local):
 
         run = call
         launches = 1
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         restore()
         run()
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
+          for _ in range(steps)]
     sampler = ClockSampler(torch.cuda.current_device())
     sampler.start()
     time.sleep(0.3)
-    for i in range(args.steps):
+    for i in range(steps):
         restore()
         ev[i][0].record(stream)
         run()
@@ -848,8 +1005,8 @@ def main_extra(args, rank, world, local):
     clocks = sampler.stop()
     total_ms = sum(a.elapsed_time(b) for a, b in ev)
     total_ms = max_over_ranks(torch, pg, total_ms, dev)
-    ms = total_ms / args.steps
-    peaks = load_peaks()
+    ms = total_ms / steps
+    peaks = ctx.peaks
     gbs = w.bytes_total / (ms / 1e3) / 1e9
     # accuracy and the comparison arm
     if w.name == "vbatched_4096":
@@ -960,7 +1117,7 @@ def main_extra(args, rank, world, local):
         e2e_step()
     torch.cuda.synchronize()
     a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    k = max(3, min(args.steps, 5))
+    k = max(3, min(steps, 5))
     a.record(stream)
     for _ in range(k):
         e2e_step()
@@ -969,86 +1126,38 @@ def main_extra(args, rank, world, local):
     e2e_ms = a.elapsed_time(b2) / k
     e2e_ms = max_over_ranks(torch, pg, e2e_ms, dev)
     line = {"metric": w.metric, "value": bc * world / (ms / 1e3), "unit": w.unit,
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": getattr(w, "dtype", "f64"),
             "data": "synthetic (seeded, generated on device)", "config": w.config,
-            "gpu_launches": launches * args.steps,
+            "gpu_launches": launches * steps,
             "e2e": {"value": bc * world / (e2e_ms / 1e3), "unit": w.unit,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "pipeline": e2e_pipeline},
-            "roofline": {"bound": "hbm", "kernel": "vb_persistent_kernel<double>"
+            "roofline": {"bound": "hbm", "limiter": "latency: per-column chains of the CTA LU",
+                         "kernel": "vb_persistent_kernel<double>"
                          if w.name == "vbatched_4096" else
                          f"solve_adjoint_kernel<{'float' if w.prec == 's' else 'double'}>",
                          "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": gbs / peaks["hbm_gbs"],
                          "traffic": w.traffic_per_unit * bc,
                          "peak_source": peaks["source"],
-                         "fp64_tflops": w.flops_total / (ms / 1e3) / 1e12},
+                         "compute": {"achieved_tflops": w.flops_total / (ms / 1e3) / 1e12,
+                                     "peak_tflops": peaks["fp64_tflops"],
+                                     "frac": w.flops_total / (ms / 1e3) / 1e12
+                                     / peaks["fp64_tflops"],
+                                     "peak": "FP64 dgemm measured in this run (cuBLAS 8192^3); "
+                                             "the FP32 adjoint is also compared with it"}},
             "clocks": clocks}
     line.update(extra)
     if rank == 0 and world == 1:
-        line["cpu_baseline"] = cpu_sample_extra(w, args.cpu_seconds)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+        line["cpu_baseline"] = cpu_sample(w, cpu_seconds)
     del graph
     torch.cuda.synchronize()
     for hh in extra_handles:
         hh.close()
-    handle.close()
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
-
-
-def cpu_sample_extra(w, target_s):
-    """The oracle on the host cores for the extra rows: per-member gesv (variable size,
-    members split over threads by the oracle) or getrs with trans = T plus the rank-nrhs
-    product (adjoint), on a bounded sample."""
-    import oracle
-    threads = oracle.nthreads_default()
-    if w.name == "vbatched_4096":
-        if not hasattr(w, "host"):
-            w.host = (w.sizes.cpu().numpy(), w.rhs.cpu().numpy(), w.A0.cpu().numpy(),
-                      w.B0.cpu().numpy())
-        sz, kk, A0, B0 = w.host
-        t0 = time.perf_counter()
-        done = 0
-        while time.perf_counter() - t0 < target_s and done < w.bc:
-            b = done
-            n, k = int(sz[b]), int(kk[b])
-            A = np.ascontiguousarray(A0[b][:n, :n]).reshape(-1)  # column-major n x n, ld n
-            Bm = np.ascontiguousarray(B0[b][:k, :n]).reshape(-1)
-            ipiv = np.zeros(n, np.int32)
-            info = np.zeros(1, np.int32)
-            oracle.gesv(n, k, A, n, n * n, ipiv, n, Bm, n, n * k, info, 1, nthreads=1)
-            done += 1
-        t = time.perf_counter() - t0
-        return {"value": done / t, "unit": w.unit, "cores": 1, "kind": "port",
-                "sample": f"first {done} of {w.bc} members, oracle gesv one member per call "
-                          f"(1 thread), {t:.1f} s"}
-    n, nrhs = w.n, w.nrhs
-    cnt = min(w.bc, 2048)
-    A = w.A0[:cnt].double().cpu().numpy().reshape(-1).copy()
-    ipiv = np.zeros(cnt * n, np.int32)
-    info = np.zeros(cnt, np.int32)
-    oracle.getrf(n, n, A, n, n * n, ipiv, n, info, cnt, nthreads=threads)
-    X = w.X0[:cnt].double().cpu().numpy()
-    G = w.G0[:cnt].double().cpu().numpy().reshape(-1)
-    reps = 0
-    t0 = time.perf_counter()
-    while True:
-        gB = G.copy()
-        oracle.getrs(1, n, nrhs, A, n, n * n, ipiv, n, gB, n, n * nrhs, cnt, nthreads=threads)
-        gBm = gB.reshape(cnt, nrhs, n)
-        _ = -np.einsum("bcr,bcj->brj", gBm, X)
-        reps += 1
-        if time.perf_counter() - t0 >= target_s:
-            break
-    t = time.perf_counter() - t0
-    return {"value": reps * cnt / t, "unit": w.unit, "cores": threads, "kind": "port",
-            "sample": f"{cnt} of {w.bc} members x {reps}, oracle getrs (trans) with "
-                      f"{threads} pthreads + numpy outer product, {t:.1f} s"}
+    del w
+    return line
 
 
 if __name__ == "__main__":

@@ -92,3 +92,105 @@ def refgen(count):
     out = np.empty(count, dtype=np.float64)
     lib().refgen_fill(_ptr(out), count)
     return out
+
+
+# ---------------------------------------------------------------------------------------
+# Host LAPACK (OpenBLAS as bundled with scipy, loaded with dlopen by oracle/lapack_host.c):
+# the reference's own CPU path for these routines, timed as the CPU baseline.  One LAPACK
+# call per member on one thread, the batch split statically over nthreads pthreads.
+LH_GETRF_GETRS, LH_POTRF_POTRS, LH_GESV, LH_DSGESV, LH_ADJOINT, LH_GETRI, LH_VGESV = range(7)
+_lh_ready = False
+
+
+def lapack_library_path():
+    """Path of scipy's bundled OpenBLAS (libscipy_openblas*.so), or None."""
+    import glob
+    try:
+        import scipy
+    except ImportError:
+        return None
+    d = os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), "scipy.libs")
+    cands = sorted(glob.glob(os.path.join(d, "libscipy_openblas*.so")))
+    return cands[0] if cands else None
+
+
+def lapack_available():
+    global _lh_ready
+    if _lh_ready:
+        return True
+    path = lapack_library_path()
+    if path is None:
+        return False
+    l = lib()
+    l.lapack_host_open.restype = ctypes.c_int
+    l.lapack_host_open.argtypes = [ctypes.c_char_p]
+    l.lapack_host_batch.restype = ctypes.c_int
+    l.lapack_host_batch.argtypes = [
+        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
+        ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
+        ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    l.lapack_host_outer.restype = ctypes.c_int
+    l.lapack_host_outer.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    _lh_ready = l.lapack_host_open(path.encode()) == 0
+    return _lh_ready
+
+
+def lapack_library_name():
+    path = lapack_library_path()
+    return os.path.basename(path) if path else None
+
+
+def lapack_batch(op, n, nrhs, A, lda, sA, ipiv=None, sP=0, B=None, ldb=1, sB=0, X=None, ldx=1,
+                 sX=0, info=None, iter=None, nv=None, rv=None, ld=1, bc=1, nthreads=1):
+    """Host LAPACK over members 0..bc-1 (flat float64 buffers, member b at b*stride)."""
+    if not lapack_available():
+        raise RuntimeError("host LAPACK (scipy's OpenBLAS) not available")
+    r = lib().lapack_host_batch(op, n, nrhs, _ptr(A), lda, sA, _ptr(ipiv), sP, _ptr(B), ldb, sB,
+                                _ptr(X), ldx, sX, _ptr(info), _ptr(iter), _ptr(nv), _ptr(rv), ld,
+                                bc, nthreads)
+    if r != 0:
+        raise RuntimeError("lapack_host_batch failed")
+
+
+def lapack_outer(n, nrhs, gB, X, gA, bc, nthreads=1):
+    """gA = -gB X^T per member with host dgemm (gB, X: n x nrhs, gA: n x n, ld n)."""
+    if not lapack_available():
+        raise RuntimeError("host LAPACK (scipy's OpenBLAS) not available")
+    if lib().lapack_host_outer(n, nrhs, _ptr(gB), _ptr(X), _ptr(gA), bc, nthreads) != 0:
+        raise RuntimeError("lapack_host_outer failed")
+
+
+def physical_cores():
+    """Physical cores of this host (distinct (physical id, core id) pairs in /proc/cpuinfo),
+    else the logical CPU count."""
+    try:
+        pairs, phys, core = set(), None, None
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                k, _, v = ln.partition(":")
+                k = k.strip()
+                if k == "physical id":
+                    phys = v.strip()
+                elif k == "core id":
+                    core = v.strip()
+                elif not k and phys is not None and core is not None:
+                    pairs.add((phys, core))
+                    phys = core = None
+        if phys is not None and core is not None:
+            pairs.add((phys, core))
+        return len(pairs) or nthreads_default()
+    except OSError:
+        return nthreads_default()
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None

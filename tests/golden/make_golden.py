@@ -14,6 +14,11 @@ bundled with scipy (scipy.linalg.lapack).  This script runs it on
     potf2_potrf_gtest.cpp, potrs_gtest.cpp, gesv_gtest.cpp, posv_gtest.cpp);
   * uniform[-1,1] matrices at the sizes of the benchmarked configurations
     (scaled down in batch), and edge sizes n = 1, 2, 31, 33, 63, 65;
+  * large members at the benchmarked orders (uniform n = 256 and 512, and the
+    mixed-precision configuration's cond-graded matrices at n = 256): ipiv and
+    info in full, the factors as projections (LU V, W^T LU for seeded Gaussian
+    V, W; tests/refcases.py projections) so the fixture stays small, and an
+    nrhs = 4 solve at n = 256;
 
 and stores the LAPACK outputs in lapack_golden.npz (the inputs are regenerated
 from the same seeded generators in tests/refcases.py).  Run it with
@@ -29,7 +34,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from tests.refcases import (ref_getrf_input, ref_getrs_input, ref_potrf_input,  # noqa: E402
-                            ref_gesv_input, uniform_general, spd_gram)
+                            ref_gesv_input, uniform_general, spd_gram, cond_graded,
+                            projections)
 
 BC = 3  # batched variants of the reference suites use batch_count = 3
 
@@ -141,6 +147,32 @@ def main():
                 out[key + "_X"] = np.stack(xs)
                 out[key + "_info"] = np.array(infos, np.int32)
                 cases.append(key)
+
+    # ---- large members: ipiv / info in full, factors as projections
+    big = [("bigrf_uni_n256", uniform_general(256, 256, 2, seed=1256)),
+           ("bigrf_uni_n512", uniform_general(512, 512, 1, seed=1512)),
+           ("bigrf_cond_n256", cond_graded(256, 3, seed=2256))]
+    for key, A in big:
+        pivs, infos, ps, qs = [], [], [], []
+        for b in range(A.shape[0]):
+            lu, piv, info = lapack_getrf(A[b])
+            p, q, _, _ = projections(lu)
+            pivs.append(piv); infos.append(info); ps.append(p); qs.append(q)
+        out[key + "_ipiv"] = np.stack(pivs)
+        out[key + "_info"] = np.array(infos, np.int32)
+        out[key + "_P"] = np.stack(ps)
+        out[key + "_Q"] = np.stack(qs)
+        cases.append(key)
+    A = uniform_general(256, 256, 2, seed=1256)
+    B = np.random.default_rng(1257).uniform(-1, 1, (2, 256, 4))
+    xs = []
+    for b in range(2):
+        lu, piv, info = lapack_getrf(A[b])
+        x, info2 = la.dgetrs(lu, piv - 1, B[b])
+        assert info2 == 0
+        xs.append(x)
+    out["bigrs_uni_n256_r4_X"] = np.stack(xs)
+    cases.append("bigrs_uni_n256_r4")
 
     out["cases"] = np.array(cases)
     path = os.path.join(HERE, "lapack_golden.npz")

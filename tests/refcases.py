@@ -74,6 +74,31 @@ def uniform_general(m, n, bc, seed, lo=-1.0, hi=1.0):
     return np.random.default_rng(seed).uniform(lo, hi, size=(bc, m, n))
 
 
+def cond_graded(n, bc, seed, lo=1.0, hi=6.0):
+    """A = U diag(s) V^T with U, V orthogonal (QR of Gaussians) and s log-spaced from 1 to
+    1/kappa, log10(kappa) ~ U[lo, hi] per member: the mixed-precision configuration's input
+    distribution, generated on the host with numpy."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((bc, n, n))
+    t = np.linspace(0.0, 1.0, n)
+    for b in range(bc):
+        U, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        V, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        lk = lo + (hi - lo) * rng.uniform()
+        out[b] = (U * 10.0 ** (-lk * t)[None, :]) @ V.T
+    return out
+
+
+def projections(M, seed=7, k=4):
+    """(M @ V, W^T @ M) for seeded N(0,1) V (n x k) and W (m x k): a compact fingerprint of
+    a large factor, so that golden fixtures of big members stay small."""
+    rng = np.random.default_rng(seed)
+    m, n = M.shape
+    V = rng.standard_normal((n, k))
+    W = rng.standard_normal((m, k))
+    return M @ V, W.T @ M, V, W
+
+
 def spd_gram(n, bc, seed):
     """A = G G^T + n I with G ~ N(0,1) (the Cholesky configuration's inputs)."""
     G = np.random.default_rng(seed).standard_normal((bc, n, n))

@@ -11,8 +11,9 @@ import pytest
 
 import oracle
 from tests.norms import eps_of, norm_error, norm_error_lower, norm_error_upper
-from tests.refcases import (from_colmajor, ref_gesv_input, ref_getrf_input, ref_getrs_input,
-                            ref_potrf_input, spd_gram, to_colmajor, uniform_general)
+from tests.refcases import (cond_graded, from_colmajor, projections, ref_gesv_input,
+                            ref_getrf_input, ref_getrs_input, ref_potrf_input, spd_gram,
+                            to_colmajor, uniform_general)
 
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "lapack_golden.npz"))
 CASES = [str(c) for c in GOLD["cases"]]
@@ -132,3 +133,50 @@ def test_oracle_batch_threads_agree():
     oracle.getrf(40, 40, f2, 40, 1600, p2, 40, i2, 16, nthreads=4)
     np.testing.assert_array_equal(f1, f2)
     np.testing.assert_array_equal(p1, p2)
+
+
+# ---- large members at the benchmarked orders (n = 256, 512; the mixed-precision
+# configuration's cond-graded inputs): ipiv and info exact, the factors through their
+# projections LU V and W^T LU (the fixture keeps those, not the factors)
+def _big_input(key):
+    _, kind, kv = _parse(key)
+    n = kv["n"]
+    if kind == "cond":
+        return cond_graded(n, 3, seed=2000 + n)
+    return uniform_general(n, n, 2 if n == 256 else 1, seed=1000 + n)
+
+
+@pytest.mark.parametrize("key", [c for c in CASES if c.startswith("bigrf")])
+def test_oracle_large_getrf_matches_lapack(key):
+    A = _big_input(key)
+    n = A.shape[1]
+    LU, ipiv, info = _oracle_getrf(A)
+    np.testing.assert_array_equal(ipiv, GOLD[key + "_ipiv"])
+    np.testing.assert_array_equal(info, GOLD[key + "_info"])
+    for b in range(A.shape[0]):
+        p, q, V, W = projections(LU[b])
+        nrm = np.linalg.norm(LU[b])
+        # ||LU_oracle - LU_lapack||_F <= n eps ||LU|| bounds each projection's error by
+        # n eps ||LU||_F ||V||_F
+        assert np.linalg.norm(p - GOLD[key + "_P"][b]) <= n * EPS * nrm * np.linalg.norm(V)
+        assert np.linalg.norm(q - GOLD[key + "_Q"][b]) <= n * EPS * nrm * np.linalg.norm(W)
+
+
+def test_oracle_large_getrs_matches_lapack():
+    A = uniform_general(256, 256, 2, seed=1256)
+    B = np.random.default_rng(1257).uniform(-1, 1, (2, 256, 4))
+    Af, Bf = to_colmajor(A), to_colmajor(B)
+    ipiv = np.zeros(2 * 256, np.int32)
+    info = np.zeros(2, np.int32)
+    oracle.gesv(256, 4, Af, 256, 256 * 256, ipiv, 256, Bf, 256, 256 * 4, info, 2)
+    X = from_colmajor(Bf, 2, 256, 4, 256, 256 * 4)
+    np.testing.assert_array_equal(ipiv.reshape(2, 256), GOLD["bigrf_uni_n256_ipiv"])
+    for b in range(2):
+        # the reference's n eps bound on the solution assumes its diagonally dominant inputs;
+        # for uniform members the two solutions differ by up to cond(A) times the backward
+        # error, so the test bounds the backward error by n eps and the difference by
+        # n eps cond(A)
+        kappa = np.linalg.cond(A[b], np.inf)
+        res = np.abs(A[b] @ X[b] - B[b]).max()
+        assert res <= 256 * EPS * np.abs(A[b]).sum(1).max() * np.abs(X[b]).max()
+        assert norm_error("I", GOLD["bigrs_uni_n256_r4_X"][b], X[b]) <= 256 * EPS * kappa

@@ -75,6 +75,89 @@ def test_noalloc_matches_allocating_vbatched_twice():
         h.close()
 
 
+def test_noalloc_matches_oracle_near_max_n():
+    """The no-allocation solve against the oracle directly (ipiv and info exact, backward
+    error < 10 n eps), with members up to max_n = 320 and one of order max_n itself."""
+    import oracle
+    import torch
+    from tests.norms import solve_backward_error
+    h = rs.Handle(torch.cuda.current_stream().cuda_stream)
+    try:
+        rng = np.random.default_rng(23)
+        ns = [int(x) for x in rng.integers(1, 320, 40)] + [320, 33, 1]
+        nrs = [int(x) for x in rng.integers(1, 9, len(ns))]
+        d = make_batch(torch, 29, ns, nrs)
+        A0 = d["A"].cpu().numpy().copy()
+        B0 = d["B"].cpu().numpy().copy()
+        st = solve("rocsolver_dgesv_vbatched_noalloc", h.value, d)
+        assert st == rs.SUCCESS, rs.STATUS_NAMES[st]
+        torch.cuda.synchronize()
+        P, I, X = d["P"].cpu().numpy(), d["I"].cpu().numpy(), d["B"].cpu().numpy()
+        eps = np.finfo(np.float64).eps
+        for i, (n, r) in enumerate(zip(ns, nrs)):
+            oA = A0[i, : n * n].copy()
+            oB = B0[i, : n * r].copy()
+            oP, oI = np.zeros(n, np.int32), np.zeros(1, np.int32)
+            oracle.gesv(n, r, oA, n, n * n, oP, n, oB, n, n * r, oI, 1)
+            assert I[i] == oI[0]
+            np.testing.assert_array_equal(P[i, :n], oP, err_msg=f"member {i} n={n}")
+            M = A0[i, : n * n].reshape(n, n).T
+            x = X[i, : n * r].reshape(r, n).T
+            b = B0[i, : n * r].reshape(r, n).T
+            assert solve_backward_error(M, x, b) < 10 * n * eps, (i, n)
+    finally:
+        h.close()
+
+
+def test_noalloc_edge_members_match_allocating_vbatched():
+    """Members the plan kernel must reject or that fail, and a batch of only small members
+    (no member for the CTA path): info, ipiv and B exactly those of the allocating
+    rocsolver_dgesv_vbatched.  Batch 1: n > max_n, lda < n, nrhs > max_nrhs (info -1,
+    member untouched), a singular member (info > 0, B unchanged) and valid members."""
+    import torch
+    h = rs.Handle(torch.cuda.current_stream().cuda_stream)
+    try:
+        def run(name, ns, nrs, lds, max_n, max_nrhs, singular=()):
+            d = make_batch(torch, 31, [max(x, 1) for x in ns], nrs)
+            for i in singular:  # a zero column makes the member exactly singular
+                n = ns[i]
+                d["A"][i, (n // 2) * n: (n // 2) * n + n] = 0.0
+            d["n"] = torch.tensor(ns, dtype=torch.int32, device="cuda")
+            d["ld"] = torch.tensor(lds, dtype=torch.int32, device="cuda")
+            d["nmax"], d["rmax"] = max_n, max_nrhs
+            st = rs.call(name, h.value, rs.ptr(d["n"]), rs.ptr(d["r"]), rs.ptr(d["pA"]),
+                         rs.ptr(d["ld"]), rs.ptr(d["pP"]), rs.ptr(d["pB"]), rs.ptr(d["ld"]),
+                         rs.ptr(d["I"]), max_n, max_nrhs, d["bc"])
+            assert st == rs.SUCCESS, rs.STATUS_NAMES[st]
+            torch.cuda.synchronize()
+            return d
+
+        ns = [40, 90, 50, 60, 30, 70]
+        nrs = [2, 1, 3, 20, 4, 2]
+        lds = [40, 90, 45, 60, 30, 70]   # member 2: lda 45 < n 50
+        ns_call = [40, 90, 50, 60, 30, 70]
+        ns_call[1] = 90                   # member 1: n 90 > max_n 80
+        for i in range(2):
+            ref = run("rocsolver_dgesv_vbatched", ns_call, nrs, lds, 80, 16, singular=(4,))
+            got = run("rocsolver_dgesv_vbatched_noalloc", ns_call, nrs, lds, 80, 16,
+                      singular=(4,))
+            info = got["I"].cpu().numpy()
+            assert info[1] == -1 and info[2] == -1 and info[3] == -1, info
+            assert info[4] > 0 and info[0] == 0 and info[5] == 0, info
+            for k in ("I", "P", "B", "A"):
+                assert torch.equal(got[k], ref[k]), (i, k)
+        small = [int(x) for x in np.random.default_rng(3).integers(1, 33, 70)]
+        snr = [1 + (x % 5) for x in small]
+        for i in range(2):
+            ref = run("rocsolver_dgesv_vbatched", small, snr, small, 32, 5)
+            got = run("rocsolver_dgesv_vbatched_noalloc", small, snr, small, 32, 5)
+            assert not got["I"].any()
+            for k in ("I", "P", "B", "A"):
+                assert torch.equal(got[k], ref[k]), (i, k)
+    finally:
+        h.close()
+
+
 def test_noalloc_rejects_batches_over_the_limit():
     import torch
     h = rs.Handle(torch.cuda.current_stream().cuda_stream)
