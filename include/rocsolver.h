@@ -103,6 +103,29 @@ ROCSOLVER_EXPORT rocblas_status rocblas_set_workspace(rocblas_handle handle, voi
 ROCSOLVER_EXPORT rocblas_status rocsolver_get_version_string(char* buf, size_t len);
 ROCSOLVER_EXPORT rocblas_status rocsolver_get_version_string_size(size_t* len);
 
+/* ---- multi-level logging ------------------------------------------------
+ * Replaces rocsolver-functions.h:66-119 (library/src/common/rocsolver_logger.cpp).
+ * rocsolver_log_begin opens a session whose layer mode and depth come from ROCSOLVER_LAYER
+ * (bit mask: rocblas_layer_mode_log_trace 1, _log_bench 2, _log_profile 4; 0x10 adds
+ * kernel launches) and ROCSOLVER_LEVELS (default 1); logs go to stderr, or to the files
+ * named by ROCSOLVER_LOG_PATH / ROCSOLVER_LOG_{TRACE,BENCH,PROFILE}_PATH.  Every entry point
+ * then writes a rocsolver-bench command line (bench), its trace tree (trace) or its
+ * accumulated time (profile; this waits for the handle's stream on return, so do not enable
+ * it while capturing a stream).  All return internal_error without an open session, and
+ * rocsolver_log_begin with one already open. */
+#define rocblas_layer_mode_none 0u
+#define rocblas_layer_mode_log_trace 1u
+#define rocblas_layer_mode_log_bench 2u
+#define rocblas_layer_mode_log_profile 4u
+#define rocblas_layer_mode_ex_log_kernel 0x10u
+ROCSOLVER_EXPORT rocblas_status rocsolver_log_begin(void);
+ROCSOLVER_EXPORT rocblas_status rocsolver_log_end(void);
+ROCSOLVER_EXPORT rocblas_status rocsolver_log_set_layer_mode(const rocblas_layer_mode_flags layer_mode);
+ROCSOLVER_EXPORT rocblas_status rocsolver_log_set_max_levels(const rocblas_int max_levels);
+ROCSOLVER_EXPORT rocblas_status rocsolver_log_restore_defaults(void);
+ROCSOLVER_EXPORT rocblas_status rocsolver_log_write_profile(void);
+ROCSOLVER_EXPORT rocblas_status rocsolver_log_flush_profile(void);
+
 /* ---- hot path: LU / Cholesky factor and solve ---------------------------
  * Each prototype keeps the reference's argument order and meaning exactly;
  * the comment names the reference declaration it replaces
@@ -579,6 +602,278 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dposv_strided_batched(rocblas_handle h
     const rocblas_stride strideB,
     rocblas_int* info,
     const rocblas_int batch_count);
+
+/* ---- inverse from the LU factors and the out-of-place solve --------------------
+ * getri: A (the LU factors and ipiv from getrf) is overwritten by inv(A) where info = 0;
+ * info = i > 0 when U(i,i) is the first zero diagonal entry, and A keeps its factors.
+ * getri_outofplace: C = inv(A), A unchanged.  npvt forms: factors from getrf_npvt.
+ * In-place getri needs n*n elements of workspace per member (handle workspace).
+ * gesv_outofplace: X = A^{-1} B with A overwritten by its LU factors; B unchanged. */
+/* replaces rocsolver-functions.h:9173-9186 / lapack/roclapack_getri.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri(rocblas_handle handle,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9245-9262 / lapack/roclapack_getri_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_batched(rocblas_handle handle,
+    const rocblas_int n,
+    float* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9329-9348 / lapack/roclapack_getri_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9402-9413 / lapack/roclapack_getri.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_npvt(rocblas_handle handle,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9463-9476 / lapack/roclapack_getri_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_npvt_batched(rocblas_handle handle,
+    const rocblas_int n,
+    float* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9532-9547 / lapack/roclapack_getri_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_npvt_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21380-21396 / lapack/roclapack_getri_outofplace.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    float* C,
+    const rocblas_int ldc,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:21462-21483 / lapack/roclapack_getri_outofplace_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_outofplace_batched(rocblas_handle handle,
+    const rocblas_int n,
+    float* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    float* const C[],
+    const rocblas_int ldc,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21562-21588 / lapack/roclapack_getri_outofplace_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_outofplace_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    float* C,
+    const rocblas_int ldc,
+    const rocblas_stride strideC,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21653-21667 / lapack/roclapack_getri_outofplace.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_npvt_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    float* C,
+    const rocblas_int ldc,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:21725-21741 / lapack/roclapack_getri_outofplace_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_npvt_outofplace_batched(rocblas_handle handle,
+    const rocblas_int n,
+    float* const A[],
+    const rocblas_int lda,
+    float* const C[],
+    const rocblas_int ldc,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21813-21834 / lapack/roclapack_getri_outofplace_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_npvt_outofplace_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    float* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    float* C,
+    const rocblas_int ldc,
+    const rocblas_stride strideC,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces lapack/roclapack_gesv_outofplace.cpp:106-135 (exported, not in the public header) */
+ROCSOLVER_EXPORT rocblas_status rocsolver_sgesv_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    float* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    float* B,
+    const rocblas_int ldb,
+    float* X,
+    const rocblas_int ldx,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9173-9186 / lapack/roclapack_getri.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri(rocblas_handle handle,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9245-9262 / lapack/roclapack_getri_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_batched(rocblas_handle handle,
+    const rocblas_int n,
+    double* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9329-9348 / lapack/roclapack_getri_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9402-9413 / lapack/roclapack_getri.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_npvt(rocblas_handle handle,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9463-9476 / lapack/roclapack_getri_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_npvt_batched(rocblas_handle handle,
+    const rocblas_int n,
+    double* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9532-9547 / lapack/roclapack_getri_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_npvt_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21380-21396 / lapack/roclapack_getri_outofplace.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    double* C,
+    const rocblas_int ldc,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:21462-21483 / lapack/roclapack_getri_outofplace_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_outofplace_batched(rocblas_handle handle,
+    const rocblas_int n,
+    double* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    double* const C[],
+    const rocblas_int ldc,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21562-21588 / lapack/roclapack_getri_outofplace_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_outofplace_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    double* C,
+    const rocblas_int ldc,
+    const rocblas_stride strideC,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21653-21667 / lapack/roclapack_getri_outofplace.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_npvt_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    double* C,
+    const rocblas_int ldc,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:21725-21741 / lapack/roclapack_getri_outofplace_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_npvt_outofplace_batched(rocblas_handle handle,
+    const rocblas_int n,
+    double* const A[],
+    const rocblas_int lda,
+    double* const C[],
+    const rocblas_int ldc,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21813-21834 / lapack/roclapack_getri_outofplace_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_npvt_outofplace_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    double* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    double* C,
+    const rocblas_int ldc,
+    const rocblas_stride strideC,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces lapack/roclapack_gesv_outofplace.cpp:106-135 (exported, not in the public header) */
+ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    double* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    double* B,
+    const rocblas_int ldb,
+    double* X,
+    const rocblas_int ldx,
+    rocblas_int* info);
 
 /* ---- entry points with no counterpart in the reference ------------------ */
 

@@ -15,7 +15,7 @@ from . import build as _build
 
 _lib = None
 
-OP_GETRF, OP_GETRS, OP_POTRF, OP_POTRS, OP_GESV, OP_POSV = range(6)
+OP_GETRF, OP_GETRS, OP_POTRF, OP_POTRS, OP_GESV, OP_POSV, OP_GETRI = range(7)
 
 
 def lib():
@@ -85,6 +85,12 @@ def gesv(n, nrhs, A, lda, strideA, ipiv, strideP, B, ldb, strideB, info, bc, nth
 def posv(upper, n, nrhs, A, lda, strideA, B, ldb, strideB, info, bc, nthreads=1):
     lib().oracle_batch(OP_POSV, _dbl(A), n, n, nrhs, 0, int(upper), 0, _ptr(A), lda, strideA,
                        None, 0, _ptr(B), ldb, strideB, _ptr(info), bc, nthreads)
+
+
+def getri(n, A, lda, strideA, ipiv, strideP, info, bc, pivot=True, nthreads=1):
+    """Inverse from the LU factors (LAPACK dgetri); A overwritten where info == 0."""
+    lib().oracle_batch(OP_GETRI, _dbl(A), n, n, 0, 0, 0, int(pivot), _ptr(A), lda, strideA,
+                       _ptr(ipiv), strideP, None, 0, 0, _ptr(info), bc, nthreads)
 
 
 def refgen(count):

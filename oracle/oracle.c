@@ -17,6 +17,9 @@
  *   potrs  : library/src/lapack/roclapack_potrs.hpp:87-152
  *   gesv/posv : library/src/lapack/roclapack_gesv.hpp:105-178, roclapack_posv.hpp:101-170
  *               (B is left unchanged where info > 0)
+ *   getri  : LAPACK dgetri / dtrti2 (unblocked), the reference's cpu_getri
+ *            (clients/common/lapack_host_reference.cpp; library/src/lapack/roclapack_getri.hpp:265-390
+ *            computes the same inverse by blocks)
  * Pinned against scipy's bundled OpenBLAS LAPACK by tests/golden/make_golden.py.
  *
  * Every routine exists for float (prefix s) and double (prefix d); batch
@@ -284,6 +287,69 @@
         oracle_##P##potf2(upper, n, A, lda, info);                                          \
         if(*info == 0)                                                                      \
             oracle_##P##potrs(upper, n, nrhs, A, lda, B, ldb);                              \
+    }                                                                                       \
+                                                                                            \
+    /* inverse from the LU factors, LAPACK dgetri unblocked (the reference's oracle,       \
+       clients/common/lapack_host_reference.cpp cpu_getri): dtrtri's singularity test      \
+       (info = first zero U(i,i); A untouched), inv(U) by dtrti2 (dtrmv + dscal per         \
+       column), then inv(A) L = inv(U) column by column from the right (dgemv), then the    \
+       column interchanges in reverse order.  pivot = 0: no interchanges (npvt).            \
+       work: n elements. */                                                                 \
+    void oracle_##P##getri(int n, T* A, int lda, const int* ipiv, int* info, T* work,       \
+                           int pivot)                                                       \
+    {                                                                                       \
+        *info = 0;                                                                          \
+        for(int i = 0; i < n; ++i)                                                          \
+            if(A[IDX(i, i, lda)] == (T)0)                                                   \
+            {                                                                               \
+                *info = i + 1;                                                              \
+                return;                                                                     \
+            }                                                                               \
+        for(int j = 0; j < n; ++j)                                                          \
+        {                                                                                   \
+            A[IDX(j, j, lda)] = (T)1 / A[IDX(j, j, lda)];                                   \
+            T ajj = -A[IDX(j, j, lda)];                                                     \
+            /* x = U(0:j,0:j) x for x = A(0:j, j) (dtrmv, upper, no transpose) */           \
+            for(int jj = 0; jj < j; ++jj)                                                   \
+            {                                                                               \
+                T t = A[IDX(jj, j, lda)];                                                   \
+                if(t != (T)0)                                                               \
+                {                                                                           \
+                    for(int i = 0; i < jj; ++i)                                             \
+                        A[IDX(i, j, lda)] += t * A[IDX(i, jj, lda)];                        \
+                    A[IDX(jj, j, lda)] = t * A[IDX(jj, jj, lda)];                           \
+                }                                                                           \
+            }                                                                               \
+            for(int i = 0; i < j; ++i)                                                      \
+                A[IDX(i, j, lda)] *= ajj;                                                   \
+        }                                                                                   \
+        for(int j = n - 1; j >= 0; --j)                                                     \
+        {                                                                                   \
+            for(int i = j + 1; i < n; ++i)                                                  \
+            {                                                                               \
+                work[i] = A[IDX(i, j, lda)];                                                \
+                A[IDX(i, j, lda)] = (T)0;                                                   \
+            }                                                                               \
+            for(int jj = j + 1; jj < n; ++jj)                                               \
+            {                                                                               \
+                T t = -work[jj];                                                            \
+                if(t != (T)0)                                                               \
+                    for(int i = 0; i < n; ++i)                                              \
+                        A[IDX(i, j, lda)] += t * A[IDX(i, jj, lda)];                        \
+            }                                                                               \
+        }                                                                                   \
+        if(pivot)                                                                           \
+            for(int j = n - 2; j >= 0; --j)                                                 \
+            {                                                                               \
+                int jp = ipiv[j] - 1;                                                       \
+                if(jp != j)                                                                 \
+                    for(int i = 0; i < n; ++i)                                              \
+                    {                                                                       \
+                        T t = A[IDX(i, j, lda)];                                            \
+                        A[IDX(i, j, lda)] = A[IDX(i, jp, lda)];                             \
+                        A[IDX(i, jp, lda)] = t;                                             \
+                    }                                                                       \
+            }                                                                               \
     }
 
 DEFINE_ORACLE(d, double, DBL_MIN, sqrt)
@@ -296,7 +362,7 @@ DEFINE_ORACLE(s, float, FLT_MIN, sqrtf)
  * does). */
 typedef struct
 {
-    int op; /* 0 getrf, 1 getrs, 2 potrf, 3 potrs, 4 gesv, 5 posv */
+    int op; /* 0 getrf, 1 getrs, 2 potrf, 3 potrs, 4 gesv, 5 posv, 6 getri */
     int dbl;
     int m, n, nrhs, trans, upper, pivot;
     void* A;
@@ -359,6 +425,16 @@ static void run_one(const job_t* j, int b)
         else
             oracle_sposv(j->upper, j->n, j->nrhs, (float*)A, j->lda, (float*)B, j->ldb, info);
         break;
+    case 6:
+    {
+        void* w = malloc(es * (size_t)(j->n > 0 ? j->n : 1));
+        if(j->dbl)
+            oracle_dgetri(j->n, (double*)A, j->lda, ipiv, info, (double*)w, j->pivot);
+        else
+            oracle_sgetri(j->n, (float*)A, j->lda, ipiv, info, (float*)w, j->pivot);
+        free(w);
+        break;
+    }
     }
 }
 

@@ -8,14 +8,16 @@ argument order, and offers thin helpers that pass torch CUDA tensors by device
 pointer.  There is no fallback: if the library is missing, importing ``lib()`` raises.
 
 Reference interface mirrored: library/include/rocsolver/rocsolver-functions.h
-(getrf :5139-5349, getrs :8562-8796, gesv :8872-9108, potrf :10188-10356,
-potrs :10426-10642, posv :10718-10944).
+(getrf :5139-5349, getrs :8562-8796, gesv :8872-9108, getri :9173-9547, potrf :10188-10356,
+potrs :10426-10642, posv :10718-10944, getri_outofplace :21380-21834) and
+library/src/lapack/roclapack_gesv_outofplace.cpp:106-135 (gesv_outofplace).
 """
 import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "librocsolver_b200.so")
+# the in-tree build; $ROCSOLVER_B200_LIB names another build of the same library instead
+LIB_PATH = os.environ.get("ROCSOLVER_B200_LIB") or os.path.join(_HERE, "librocsolver_b200.so")
 
 # rocblas_status
 SUCCESS, INVALID_HANDLE, NOT_IMPLEMENTED, INVALID_POINTER, INVALID_SIZE, MEMORY_ERROR, \
@@ -59,6 +61,19 @@ _SIG = {
     "posv": [E, I, I, P, I, P, I, P],
     "posv_batched": [E, I, I, P, I, P, I, P, I],
     "posv_strided_batched": [E, I, I, P, I, S, P, I, S, P, I],
+    "getri": [I, P, I, P, P],
+    "getri_batched": [I, P, I, P, S, P, I],
+    "getri_strided_batched": [I, P, I, S, P, S, P, I],
+    "getri_npvt": [I, P, I, P],
+    "getri_npvt_batched": [I, P, I, P, I],
+    "getri_npvt_strided_batched": [I, P, I, S, P, I],
+    "getri_outofplace": [I, P, I, P, P, I, P],
+    "getri_outofplace_batched": [I, P, I, P, S, P, I, P, I],
+    "getri_outofplace_strided_batched": [I, P, I, S, P, S, P, I, S, P, I],
+    "getri_npvt_outofplace": [I, P, I, P, I, P],
+    "getri_npvt_outofplace_batched": [I, P, I, P, I, P, I],
+    "getri_npvt_outofplace_strided_batched": [I, P, I, S, P, I, S, P, I],
+    "gesv_outofplace": [I, I, P, I, P, P, I, P, I, P],
 }
 
 # entry points with no counterpart in the reference (declared in include/rocsolver.h)
@@ -94,6 +109,13 @@ _HANDLE_FUNCS = {
     "rocblas_set_workspace": (_c.c_int, [H, _c.c_void_p, _c.c_size_t]),
     "rocsolver_get_version_string": (_c.c_int, [_c.c_char_p, _c.c_size_t]),
     "rocsolver_get_version_string_size": (_c.c_int, [_c.POINTER(_c.c_size_t)]),
+    "rocsolver_log_begin": (_c.c_int, []),
+    "rocsolver_log_end": (_c.c_int, []),
+    "rocsolver_log_set_layer_mode": (_c.c_int, [_c.c_uint32]),
+    "rocsolver_log_set_max_levels": (_c.c_int, [I]),
+    "rocsolver_log_restore_defaults": (_c.c_int, []),
+    "rocsolver_log_write_profile": (_c.c_int, []),
+    "rocsolver_log_flush_profile": (_c.c_int, []),
 }
 
 _lib = None

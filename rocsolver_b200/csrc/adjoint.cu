@@ -10,6 +10,7 @@
 // sweeps, and gA is written straight from that shared-memory copy of gB, so the factors
 // are read once and gA once written; no refactorisation and no workspace.
 #include "launch.h"
+#include "logger.h"
 #include "trsv.cuh"
 
 namespace rsb {
@@ -130,6 +131,7 @@ rocblas_status launch_solve_adjoint(cudaStream_t s, int kind, int n, int nrhs, B
     if(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
        != cudaSuccess)
         return rocblas_status_internal_error;
+    RSB_LOG_KERNEL("solve_adjoint_kernel");
     k<<<bc, NT, smem, s>>>(kind, n, nrhs, A, lda, ipiv, strideP, X, ldx, G, ldg, GA, ldga, GB,
                            ldgb);
     return cudaGetLastError() == cudaSuccess ? rocblas_status_success

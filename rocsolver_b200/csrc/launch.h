@@ -32,6 +32,14 @@ rocblas_status launch_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T>
                             Batch<T> B, int ldb, const int* skip_info, int bc);
 rocblas_status launch_reset_info(cudaStream_t s, int* info, int bc);
 
+// inverse from the LU factors (getri.cu): C.base == C.ptrs == nullptr means in place (the
+// inverse is formed in ws, getri_workspace bytes, and copied over A where info == 0);
+// ipiv == nullptr means no pivoting (npvt forms)
+size_t getri_workspace(int n, int bc, size_t elem, bool inplace);
+template <typename T>
+rocblas_status launch_getri(cudaStream_t s, int n, Batch<T> A, int lda, const int* ipiv,
+                            int64_t strideP, Batch<T> C, int ldc, int* info, int bc, void* ws);
+
 // mixed-precision solver (mixed.cu)
 size_t dsgesv_workspace(int n, int nrhs, int bc);
 rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, int lda,

@@ -6,6 +6,7 @@
 // run-time tuning table (tuning.h) when it has an entry, else from the built-in choice.
 #include "chol.cuh"
 #include "launch.h"
+#include "logger.h"
 #include "lu_cta.cuh"
 #include "lu_small.cuh"
 #include "trsv.cuh"
@@ -68,6 +69,7 @@ static void run_getrf_warp(cudaStream_t s, int m, int n, Batch<T> A, int lda, in
                            int64_t sP, int* info, int bc, Gate g)
 {
     dim3 grid((bc + SMALL_WPB - 1) / SMALL_WPB);
+    RSB_LOG_KERNEL("getrf_warp_kernel");
     getrf_warp_kernel<T, NMAX, PIVOT><<<grid, 32 * SMALL_WPB, 0, s>>>(m, n, A, lda, ipiv, sP,
                                                                        info, bc, g);
 }
@@ -100,6 +102,7 @@ static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, in
         return rocblas_status_internal_error;
     if(ran)
         *ran = true;
+    RSB_LOG_KERNEL("getrf_cta_kernel");
     k<<<bc, NT, smem, s>>>(m, n, A, lda, ipiv, sP, info, cw, fold, g);
     return launch_status();
 }
@@ -201,6 +204,7 @@ static void run_getrs_warp(cudaStream_t s, int trans, int n, int nrhs, Batch<T> 
 {
     const int64_t tasks = (int64_t)bc * ((nrhs + NRC - 1) / NRC);
     dim3 grid((unsigned)((tasks + SMALL_WPB - 1) / SMALL_WPB));
+    RSB_LOG_KERNEL("getrs_warp_kernel");
     getrs_warp_kernel<T, NMAX, NRC><<<grid, 32 * SMALL_WPB, 0, s>>>(trans, n, nrhs, A, lda, ipiv,
                                                                      sP, B, ldb, skip, bc, g);
 }
@@ -227,6 +231,7 @@ static rocblas_status run_getrs_cta_nt(cudaStream_t s, int trans, int n, int nrh
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
     const int64_t groups = (nrhs + NRC - 1) / NRC;
+    RSB_LOG_KERNEL("getrs_cta_kernel");
     k<<<(unsigned)(bc * groups), NT, smem, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip,
                                                 g);
     return launch_status();
@@ -274,6 +279,7 @@ static void run_gesv_warp(cudaStream_t s, int n, int nrhs, Batch<T> A, int lda, 
                           int64_t sP, Batch<T> B, int ldb, int* info, int bc)
 {
     dim3 grid((bc + SMALL_WPB - 1) / SMALL_WPB);
+    RSB_LOG_KERNEL("gesv_warp_kernel");
     if(nrhs == 1)
         gesv_warp_kernel<T, NMAX, 1><<<grid, 32 * SMALL_WPB, 0, s>>>(n, nrhs, A, lda, ipiv, sP,
                                                                       B, ldb, info, bc);
@@ -313,6 +319,7 @@ static rocblas_status run_potrf(cudaStream_t s, int upper, int n, Batch<T> A, in
     auto k = potrf_cta_kernel<T, NT, R, JB, TN>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
+    RSB_LOG_KERNEL("potrf_cta_kernel");
     k<<<bc, NT, smem, s>>>(upper, n, A, lda, info);
     return launch_status();
 }
@@ -321,6 +328,7 @@ template <typename T, int N>
 static rocblas_status run_potrf_reg(cudaStream_t s, int upper, int n, Batch<T> A, int lda,
                                     int* info, int bc)
 {
+    RSB_LOG_KERNEL("potrf_reg_kernel");
     potrf_reg_kernel<T, N><<<bc, N, 0, s>>>(upper, n, A, lda, info);
     return launch_status();
 }
@@ -353,6 +361,7 @@ static rocblas_status run_potrs_nt(cudaStream_t s, int upper, int n, int nrhs, B
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
     const int64_t groups = (nrhs + NRC - 1) / NRC;
+    RSB_LOG_KERNEL("potrs_cta_kernel");
     k<<<(unsigned)(bc * groups), NT, smem, s>>>(upper, n, nrhs, A, lda, B, ldb, skip);
     return launch_status();
 }
@@ -362,6 +371,7 @@ static rocblas_status run_potrs_small(cudaStream_t s, int upper, int n, int nrhs
                                       int lda, Batch<T> B, int ldb, const int* skip, int bc)
 {
     const int64_t groups = (nrhs + NRC - 1) / NRC;
+    RSB_LOG_KERNEL("potrs_small_kernel");
     potrs_small_kernel<T, N, NRC>
         <<<(unsigned)(bc * groups), N, 0, s>>>(upper, n, nrhs, A, lda, B, ldb, skip);
     return launch_status();

@@ -22,6 +22,7 @@
 
 #include "handle.h"
 #include "launch.h"
+#include "logger.h"
 #include "trsv.cuh"
 
 namespace rsb {
@@ -679,7 +680,10 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
     const bool refine_ok = smem <= 200 * 1024 && n <= MAX_CTA_ROWS;
     if(refine_ok)
     {
-        dsgesv_convert_kernel<<<bc, 256, 0, s>>>(n, A, lda, a32, flag, info, iter);
+        {
+            RSB_LOG_KERNEL("dsgesv_convert_kernel");
+            dsgesv_convert_kernel<<<bc, 256, 0, s>>>(n, A, lda, a32, flag, info, iter);
+        }
         if(cudaGetLastError() != cudaSuccess)
             return rocblas_status_internal_error;
         rocblas_status st = launch_getrf<float>(s, n, n, strided<float>(a32, (int64_t)n * n), n,
@@ -687,6 +691,7 @@ rocblas_status launch_dsgesv(cudaStream_t s, int n, int nrhs, Batch<double> A, i
                                                 true);
         if(st != rocblas_status_success)
             return st;
+        RSB_LOG_KERNEL("dsgesv_refine_kernel");
         if(NRC == 1)
         {
             auto k = dsgesv_refine_kernel<NT, 1>;

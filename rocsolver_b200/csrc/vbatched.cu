@@ -15,6 +15,7 @@
 // (solve) ldb < n / nrhs < 0 / nrhs > max_nrhs gets info = -1 and is left untouched.
 #include "handle.h"
 #include "launch.h"
+#include "logger.h"
 #include "tuning.h"
 #include "lu_cta.cuh"
 #include "lu_small.cuh"
@@ -274,6 +275,7 @@ static rocblas_status run_vb(cudaStream_t s, VbArgs v, T* const* A, T* const* B,
         grid = v.bc;
     if(ran)
         *ran = true;
+    RSB_LOG_KERNEL("vb_persistent_kernel");
     k<<<grid, NT, smem, s>>>(v, A, B, cw, fold);
     return cudaGetLastError() == cudaSuccess ? rocblas_status_success
                                              : rocblas_status_internal_error;
@@ -300,7 +302,10 @@ rocblas_status launch_vbatched(cudaStream_t s, int mode, const int* n, const int
     v.info = info;
     v.order = static_cast<int*>(ws);
     v.counters = reinterpret_cast<int*>(static_cast<char*>(ws) + ws_round(sizeof(int) * bc));
-    vb_plan_kernel<<<1, 1024, sizeof(int) * (max_n + 2), s>>>(v);
+    {
+        RSB_LOG_KERNEL("vb_plan_kernel");
+        vb_plan_kernel<<<1, 1024, sizeof(int) * (max_n + 2), s>>>(v);
+    }
     if(cudaGetLastError() != cudaSuccess)
         return rocblas_status_internal_error;
     VbCfg c;

@@ -22,6 +22,7 @@
 
 #include "handle.h"
 #include "launch.h"
+#include "logger.h"
 
 namespace rsb {
 namespace {
@@ -68,6 +69,8 @@ extern "C" rocblas_status rocsolver_dgesv_vbatched_noalloc(
     const rocblas_int* ldb, rocblas_int* info, const rocblas_int max_n,
     const rocblas_int max_nrhs, const rocblas_int batch_count)
 {
+    RSB_LOG_TOP('d', "gesv_vbatched_noalloc", logging::arg("--max_n", max_n),
+                logging::arg("--max_nrhs", max_nrhs), logging::arg("--batch_count", batch_count));
     if(!handle)
         return rocblas_status_invalid_handle;
     if(max_n < 0 || max_nrhs < 0 || batch_count < 0 || batch_count > VB_NOALLOC_MAX_BATCH)

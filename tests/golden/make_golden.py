@@ -14,6 +14,11 @@ bundled with scipy (scipy.linalg.lapack).  This script runs it on
     potf2_potrf_gtest.cpp, potrs_gtest.cpp, gesv_gtest.cpp, posv_gtest.cpp);
   * uniform[-1,1] matrices at the sizes of the benchmarked configurations
     (scaled down in batch), and edge sizes n = 1, 2, 31, 33, 63, 65;
+  * getri on the reference's getri inputs (testing_getri.hpp:102-166: the host
+    getrf factors of a scaled, row-reversed integer matrix, with zeroed U
+    diagonal entries in the singular members) over its check-in sizes
+    (clients/gtest/getri_gtest.cpp:24-37): the factors and pivots given to
+    getri, and the inverse and info LAPACK dgetri returns;
   * large members at the benchmarked orders (uniform n = 256 and 512, and the
     mixed-precision configuration's cond-graded matrices at n = 256): ipiv and
     info in full, the factors as projections (LU V, W^T LU for seeded Gaussian
@@ -35,7 +40,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from tests.refcases import (ref_getrf_input, ref_getrs_input, ref_potrf_input,  # noqa: E402
                             ref_gesv_input, uniform_general, spd_gram, cond_graded,
-                            projections)
+                            projections, ref_getri_matrix, ref_getri_singular)
 
 BC = 3  # batched variants of the reference suites use batch_count = 3
 
@@ -147,6 +152,26 @@ def main():
                 out[key + "_X"] = np.stack(xs)
                 out[key + "_info"] = np.array(infos, np.int32)
                 cases.append(key)
+
+    # ---- getri: reference suite (n, singular) with lda = n
+    for n, singular in ((32, False), (50, True), (70, False), (100, True)):
+        A = ref_getri_matrix(n, n, BC)
+        lus, pivs, invs, infos = [], [], [], []
+        for b in range(BC):
+            lu, piv, info = lapack_getrf(A[b])
+            assert info == 0
+            if singular:
+                for i in ref_getri_singular(b, BC, n):
+                    lu[i, i] = 0.0
+            inv, info2 = la.dgetri(lu, piv - 1)
+            lus.append(lu); pivs.append(piv); infos.append(int(info2))
+            invs.append(inv if info2 == 0 else lu)
+        key = f"getri_ref_n{n}_s{int(singular)}"
+        out[key + "_LU"] = np.stack(lus)
+        out[key + "_ipiv"] = np.stack(pivs)
+        out[key + "_inv"] = np.stack(invs)
+        out[key + "_info"] = np.array(infos, np.int32)
+        cases.append(key)
 
     # ---- large members: ipiv / info in full, factors as projections
     big = [("bigrf_uni_n256", uniform_general(256, 256, 2, seed=1256)),

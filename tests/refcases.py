@@ -70,6 +70,26 @@ def ref_potrf_input(n, bc, singular):
     return A
 
 
+def ref_getri_matrix(n, lda, bc):
+    """clients/include/testing_getri.hpp:102-150 before its host getrf: integers 1..10 scaled
+    to v/10 + 10 on the diagonal and (v - 4)/10 off it, rows reversed."""
+    A = _member_view(_refstream(bc * lda * n), bc, lda, n)[:, :n, :].copy()
+    idx = np.arange(n)
+    for b in range(bc):
+        M = (A[b] - 4.0) / 10.0
+        M[idx, idx] = A[b][idx, idx] / 10.0 + 10.0
+        A[b] = M[::-1, :]
+    return A
+
+
+def ref_getri_singular(b, bc, n):
+    """Diagonal positions of U zeroed in the reference's singular getri members
+    (testing_getri.hpp:150-166), or () for a regular member."""
+    if b == bc // 4 or b == bc // 2 or b == bc - 1:
+        return tuple(sorted({(n // 4 + b) % n, (n // 2 + b) % n, (n - 1 + b) % n}))
+    return ()
+
+
 def uniform_general(m, n, bc, seed, lo=-1.0, hi=1.0):
     return np.random.default_rng(seed).uniform(lo, hi, size=(bc, m, n))
 

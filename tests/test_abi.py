@@ -165,6 +165,62 @@ def test_potrf_potrs_posv_bad_args(handle, p):
     assert rs.call(v, handle, rs.FILL_LOWER, 1, 1, FAKE, 1, 1, FAKE, 1, 1, NULL, 0) == rs.SUCCESS
 
 
+@pytest.mark.parametrize("p", ["s", "d"])
+def test_getri_bad_args(handle, p):
+    """clients/include/testing_getri.hpp:15-88 and testing_getri_outofplace.hpp bad-arg
+    order: handle, sizes (n, lda, ldc, bc), then pointers (A, C, ipiv unless npvt, info)."""
+    f = f"rocsolver_{p}getri_strided_batched"
+    ok = dict(n=1, A=FAKE, lda=1, sA=1, ipiv=FAKE, sP=1, info=FAKE, bc=1)
+
+    def c(h=handle, **kw):
+        a = dict(ok, **kw)
+        return rs.call(f, h, a["n"], a["A"], a["lda"], a["sA"], a["ipiv"], a["sP"], a["info"],
+                       a["bc"])
+    assert c(h=None) == rs.INVALID_HANDLE
+    assert c(n=-1) == rs.INVALID_SIZE
+    assert c(n=2, lda=1) == rs.INVALID_SIZE
+    assert c(bc=-1) == rs.INVALID_SIZE
+    assert c(n=-1, A=NULL) == rs.INVALID_SIZE
+    for k in ("A", "ipiv", "info"):
+        assert c(**{k: NULL}) == rs.INVALID_POINTER, k
+    assert c(bc=0, info=NULL) == rs.SUCCESS
+    assert rs.call(f"rocsolver_{p}getri_npvt_strided_batched", handle, 1, FAKE, 1, 1, NULL, 1) \
+        == rs.INVALID_POINTER
+    g = f"rocsolver_{p}getri_outofplace_strided_batched"
+    # n, A, lda, sA, ipiv, sP, C, ldc, sC, info, bc
+    assert rs.call(g, handle, 2, FAKE, 2, 4, FAKE, 2, FAKE, 1, 4, FAKE, 1) == rs.INVALID_SIZE
+    assert rs.call(g, handle, 1, FAKE, 1, 1, FAKE, 1, NULL, 1, 1, FAKE, 1) == rs.INVALID_POINTER
+    assert rs.call(g, handle, 1, FAKE, 1, 1, NULL, 1, FAKE, 1, 1, FAKE, 1) == rs.INVALID_POINTER
+    assert rs.call(f"rocsolver_{p}getri_npvt_outofplace_strided_batched", handle, 1, FAKE, 1, 1,
+                   FAKE, 1, 1, NULL, 1) == rs.INVALID_POINTER
+    # in-place getri reports its workspace (n*n elements per member) to a size query
+    sz = ctypes.c_size_t()
+    assert rs.call("rocblas_start_device_memory_size_query", handle) == rs.SUCCESS
+    assert c(n=64, lda=64, sA=4096, sP=64, bc=10) == rs.SIZE_INCREASED
+    assert rs.call("rocblas_stop_device_memory_size_query", handle, ctypes.byref(sz)) \
+        == rs.SUCCESS
+    assert sz.value >= 64 * 64 * 10 * (8 if p == "d" else 4)
+
+
+@pytest.mark.parametrize("p", ["s", "d"])
+def test_gesv_outofplace_bad_args(handle, p):
+    """clients/include/testing_gesv_outofplace.hpp:15-90 bad-arg order."""
+    f = f"rocsolver_{p}gesv_outofplace"
+    ok = dict(n=1, r=1, A=FAKE, lda=1, ipiv=FAKE, B=FAKE, ldb=1, X=FAKE, ldx=1, info=FAKE)
+
+    def c(h=handle, **kw):
+        a = dict(ok, **kw)
+        return rs.call(f, h, a["n"], a["r"], a["A"], a["lda"], a["ipiv"], a["B"], a["ldb"],
+                       a["X"], a["ldx"], a["info"])
+    assert c(h=None) == rs.INVALID_HANDLE
+    assert c(n=-1) == rs.INVALID_SIZE
+    assert c(r=-1) == rs.INVALID_SIZE
+    assert c(n=2, lda=1, ldb=2, ldx=2) == rs.INVALID_SIZE
+    assert c(n=2, lda=2, ldb=2, ldx=1) == rs.INVALID_SIZE
+    for k in ("A", "ipiv", "B", "X", "info"):
+        assert c(**{k: NULL}) == rs.INVALID_POINTER, k
+
+
 def test_memory_model_defaults_and_query(handle):
     """clients/gtest/memory_model_gtest.cpp:54-120: managed by default, 32 MiB nominal,
     a size query reports without computing and returns the size on stop."""

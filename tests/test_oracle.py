@@ -180,3 +180,23 @@ def test_oracle_large_getrs_matches_lapack():
         res = np.abs(A[b] @ X[b] - B[b]).max()
         assert res <= 256 * EPS * np.abs(A[b]).sum(1).max() * np.abs(X[b]).max()
         assert norm_error("I", GOLD["bigrs_uni_n256_r4_X"][b], X[b]) <= 256 * EPS * kappa
+
+
+@pytest.mark.parametrize("key", [c for c in CASES if c.startswith("getri")])
+def test_oracle_getri_matches_lapack(key):
+    """Inverse from the reference's getri inputs: info exact, inverse within n*eps (F-norm,
+    clients/include/testing_getri.hpp:209-233)."""
+    _, _, kv = _parse(key)
+    n = kv["n"]
+    LU = GOLD[key + "_LU"]
+    flat = to_colmajor(LU)
+    ipiv = GOLD[key + "_ipiv"].astype(np.int32).reshape(-1).copy()
+    info = np.zeros(3, np.int32)
+    oracle.getri(n, flat, n, n * n, ipiv, n, info, 3)
+    np.testing.assert_array_equal(info, GOLD[key + "_info"])
+    inv = from_colmajor(flat, 3, n, n, n, n * n)
+    for b in range(3):
+        if info[b] == 0:
+            assert norm_error("F", GOLD[key + "_inv"][b], inv[b]) <= n * EPS
+        else:  # LAPACK leaves the factors in place
+            np.testing.assert_array_equal(inv[b], LU[b])
