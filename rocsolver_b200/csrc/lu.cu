@@ -78,7 +78,7 @@ static void run_getrf_warp(cudaStream_t s, int m, int n, Batch<T> A, int lda, in
 // most, so that two CTAs fit in an SM's shared memory).  *ran = false when the variant
 // cannot take this size (more rows than threads x rows per thread, or too much shared
 // memory): the caller then uses the built-in choice.
-template <typename T, int NT, int R, int JB, bool PIVOT, bool TC = false>
+template <typename T, int NT, int R, int JB, bool PIVOT, bool TC = false, bool UM = false>
 static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, int lda,
                                     int* ipiv, int64_t sP, int* info, int bc, Gate g, int cw,
                                     int fold, bool* ran = nullptr)
@@ -94,10 +94,14 @@ static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, in
     cw = ((cw + 31) / 32) * 32;
     if(cw > nround)
         cw = nround;
-    const size_t smem = CtaLuSmem<T, NT, JB>::bytes(m, cw, R);
+    if(UM && cw > 256) // one MMA covers at most 256 columns
+        cw = 256;
+    size_t smem = CtaLuSmem<T, NT, JB>::bytes(m, cw, R);
+    if constexpr(UM)
+        smem += um_bytes<NT, JB>(cw);
     if(smem > 227 * 1024)
         return rocblas_status_not_implemented;
-    auto k = getrf_cta_kernel<T, NT, R, JB, 8, PIVOT, TC>;
+    auto k = getrf_cta_kernel<T, NT, R, JB, 8, PIVOT, TC, UM>;
     if(!set_smem(k, smem))
         return rocblas_status_internal_error;
     if(ran)
@@ -114,6 +118,29 @@ static rocblas_status run_getrf_tuned(const LuCfg& c, cudaStream_t s, int m, int
                                       int bc, Gate g, bool* ran)
 {
     *ran = false;
+    // fold = 2 selects the tcgen05 trailing update (FP32 split-TF32 variants, panel widths
+    // that are multiples of 8)
+    if constexpr(sizeof(T) == 4 && TC && PIVOT)
+    {
+        if(c.fold == 2)
+        {
+#define RSB_LU_UM_VARIANT(NT_, R_, JB_)                                                        \
+            if(c.nt == NT_ && c.r == R_ && c.jb == JB_)                                        \
+                return run_getrf_cta<T, NT_, R_, JB_, PIVOT, TC, true>(s, m, n, A, lda, ipiv, \
+                                                                       sP, info, bc, g, c.cw, 0, \
+                                                                       ran);
+            RSB_LU_UM_VARIANT(128, 1, 32)
+            RSB_LU_UM_VARIANT(128, 2, 32)
+            RSB_LU_UM_VARIANT(256, 1, 32)
+            RSB_LU_UM_VARIANT(256, 2, 32)
+            RSB_LU_UM_VARIANT(256, 2, 16)
+            RSB_LU_UM_VARIANT(256, 4, 16)
+            RSB_LU_UM_VARIANT(256, 4, 8)
+            RSB_LU_UM_VARIANT(256, 8, 8)
+#undef RSB_LU_UM_VARIANT
+            return rocblas_status_not_implemented;
+        }
+    }
 #define RSB_LU_VARIANT(NT_, R_, JB_)                                                          \
     if(c.nt == NT_ && c.r == R_ && c.jb == JB_)                                                \
         return run_getrf_cta<T, NT_, R_, JB_, PIVOT, TC>(s, m, n, A, lda, ipiv, sP, info, bc, \

@@ -29,6 +29,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "umma.cuh"
 
 namespace rsb {
 
@@ -72,6 +73,42 @@ struct CtaLuSmem
         s += sizeof(int) * (JB + 2);            // panel pivots, counter
         return (s + 15) & ~size_t(15);
     }
+};
+
+// Shared memory of the tcgen05 trailing update (UM variants), placed after CtaLuSmem's
+// region (1024-byte aligned): A operand tiles of L21 (groups of um_group() M-tiles of 128
+// rows, split TF32 hi and lo), the B operand (a U12 column chunk, hi and lo), an mbarrier and
+// the TMEM base address.  One M-tile group's accumulators take um_group() * cw TMEM columns.
+template <int NT, int JB>
+__host__ __device__ constexpr int um_group_max()
+{
+    return NT <= 128 ? 1 : (JB >= 32 ? 2 : 4);
+}
+template <int NT, int JB>
+__host__ __device__ inline int um_group(int cw)
+{
+    const int g = um_group_max<NT, JB>();
+    return g * cw <= 512 ? g : (512 / cw > 0 ? 512 / cw : 1);
+}
+template <int NT, int JB>
+__host__ __device__ inline size_t um_bytes(int cw)
+{
+    return 1024 + sizeof(float) * (size_t)(2 * um_group_max<NT, JB>() * 128 * JB + 2 * cw * JB)
+           + 64;
+}
+
+// State of the tcgen05 trailing update for one CTA
+struct UmCtx
+{
+    float* ahi;       // [G][128 x JB] K-major split-TF32 tiles of L21
+    float* alo;
+    float* bhi;       // [cw x JB] K-major split-TF32 U12 chunk
+    float* blo;
+    uint64_t* mbar;   // MMA completion
+    uint32_t tmem;    // TMEM base (G * cw columns)
+    int G;
+    uint32_t phase;
+    int failed;       // an MMA completion wait ran out (CTA-uniform)
 };
 
 // ---------------------------------------------------------------------------------------
@@ -330,17 +367,139 @@ struct TileOf<float, true>
     using type = WarpTileTF32;
 };
 
+// A22 += L21 U12 on tcgen05 for one panel (rows already interchanged in memory, U12 stored in
+// the panel's top rows j0..j0+jb-1).  A22 = rows j0+jb.. (mt of them), columns j0+jb..n-1.
+// sP holds -L by slot ([k][slot], leading dimension ldp); A22 row r takes L21 row slotof[jb+r].
+// M-tiles of 128 rows are processed G at a time: their split-TF32 L21 tiles are built once,
+// then for each column chunk of at most cw columns the U12 chunk is split into the B operand,
+// one thread issues 3 * (JB/8) MMAs per M-tile into TMEM (columns t*cw.. of tile t), commits
+// to the mbarrier, and after the (bounded) wait every warp adds its TMEM rows into A22 with
+// coalesced column accesses (warp w reads TMEM lanes 32*(w%4)..+31 of the tiles of its
+// warpgroup).  All threads of the CTA call it.
+template <int NT, int JB>
+__device__ __noinline__ void umma_update(float* a, int lda, int j0, int jb, int mt, int n,
+                                         const float* sP, int ldp, const int* slotof, int cw,
+                                         UmCtx& um)
+{
+    const int c_first = j0 + jb;
+    if(mt <= 0 || c_first >= n || um.failed)
+        return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int TILE = 128 * JB;          // floats per M-tile operand
+    constexpr uint32_t SBO = (JB / 4) * 128; // bytes between 8-row groups
+    const int mtiles = (mt + 127) / 128;
+    const int G = um.G;
+    const uint32_t ahi = umma::smem_u32(um.ahi), alo = umma::smem_u32(um.alo);
+    const uint32_t bhi = umma::smem_u32(um.bhi), blo = umma::smem_u32(um.blo);
+    for(int g0 = 0; g0 < mtiles && !um.failed; g0 += G)
+    {
+        const int gt = min(G, mtiles - g0);
+        // L21 tiles of this group: row r (A22 position jb + r) from slot slotof[jb + r]
+        for(int e = tid; e < gt * 128 * JB; e += NT)
+        {
+            const int rr = e % (gt * 128), k = e / (gt * 128);
+            const int t = rr >> 7, rl = rr & 127, r = g0 * 128 + rr;
+            const float x = (r < mt && k < jb) ? sP[k * ldp + slotof[jb + r]] : 0.f;
+            uint32_t h, l;
+            umma::split_tf32(x, h, l);
+            const uint32_t off = umma::kmaj_off(rl, k, JB) >> 2;
+            reinterpret_cast<uint32_t*>(um.ahi + t * TILE)[off] = h;
+            reinterpret_cast<uint32_t*>(um.alo + t * TILE)[off] = l;
+        }
+        for(int c0 = c_first; c0 < n && !um.failed; c0 += cw)
+        {
+            const int ncol = min(cw, n - c0);
+            const int ncp = (ncol + 31) & ~31;
+            // U12 chunk (the panel's top rows, just stored) -> B operand
+            for(int e = tid; e < ncp * JB; e += NT)
+            {
+                const int k = e % JB, col = e / JB;
+                const float x = (k < jb && col < ncol) ? a[ix(j0 + k, c0 + col, lda)] : 0.f;
+                uint32_t h, l;
+                umma::split_tf32(x, h, l);
+                const uint32_t off = umma::kmaj_off(col, k, JB) >> 2;
+                reinterpret_cast<uint32_t*>(um.bhi)[off] = h;
+                reinterpret_cast<uint32_t*>(um.blo)[off] = l;
+            }
+            umma::fence_async_shared();
+            umma::fence_before_sync();
+            __syncthreads();
+            umma::fence_after_sync();
+            if(tid == 0)
+            {
+                const uint32_t idesc = umma::idesc_tf32(128, ncp);
+                for(int t = 0; t < gt; ++t)
+                {
+                    const uint32_t d = um.tmem + (uint32_t)(t * cw);
+#pragma unroll
+                    for(int s = 0; s < JB / 8; ++s)
+                    {
+                        const uint32_t ao = (uint32_t)(t * TILE * 4 + 256 * s), bo = 256u * s;
+                        umma::mma_tf32(d, umma::sdesc(alo + ao, 128, SBO),
+                                       umma::sdesc(bhi + bo, 128, SBO), idesc, s > 0 ? 1u : 0u);
+                        umma::mma_tf32(d, umma::sdesc(ahi + ao, 128, SBO),
+                                       umma::sdesc(blo + bo, 128, SBO), idesc, 1u);
+                        umma::mma_tf32(d, umma::sdesc(ahi + ao, 128, SBO),
+                                       umma::sdesc(bhi + bo, 128, SBO), idesc, 1u);
+                    }
+                }
+                umma::commit(um.mbar);
+            }
+            const bool ok = umma::mbar_wait(um.mbar, um.phase);
+            um.phase ^= 1u;
+            if(__syncthreads_or(ok ? 0 : 1))
+            {
+                um.failed = 1;
+                break;
+            }
+            umma::fence_after_sync();
+            // epilogue: A22 rows of this warp's TMEM lanes += their accumulators
+            for(int t = warp >> 2; t < gt; t += NT / 128)
+            {
+                const int row = (g0 + t) * 128 + (warp & 3) * 32 + lane;
+                for(int cb = 0; cb < ncp; cb += 16)
+                {
+                    float v[16];
+                    umma::tmem_ld16(um.tmem + ((uint32_t)((warp & 3) * 32) << 16)
+                                        + (uint32_t)(t * cw + cb),
+                                    v);
+                    if(row < mt)
+                    {
+                        float* dst = a + ix(j0 + jb + row, c0 + cb, lda);
+                        float old[16];
+#pragma unroll
+                        for(int j = 0; j < 16; ++j)
+                            old[j] = cb + j < ncol ? dst[(size_t)j * lda] : 0.f;
+#pragma unroll
+                        for(int j = 0; j < 16; ++j)
+                            if(cb + j < ncol)
+                                dst[(size_t)j * lda] = old[j] + v[j];
+                    }
+                }
+            }
+            umma::fence_before_sync();
+            __syncthreads(); // the B operand and TMEM are reused by the next chunk
+        }
+    }
+}
+
 // Factor one m x n matrix with the whole CTA.  smem_raw must hold CtaLuSmem::bytes(m, cw, R);
 // m <= R*NT; cw is a multiple of 32.  Writes ipiv (1-based, PIVOT only) and *info_out.
 // fold: apply each panel's row interchanges to the columns right of it inside the trailing
 // update instead of swapping them in memory first (a tuning choice; same results).
 // TC: FP32 trailing products on the split-TF32 tensor path (WarpTileTF32).
 // Called by all threads of the CTA.
-template <typename T, int NT, int R, int JB, int TN, bool PIVOT, bool TC = false>
+// UM (FP32 with TC and PIVOT, JB a multiple of 8): the trailing update A22 += L21 U12 runs
+// on tcgen05 (umma_update below) with the rows interchanged in memory first (no fold) and
+// U12 stored before it; um holds its buffers and TMEM.
+template <typename T, int NT, int R, int JB, int TN, bool PIVOT, bool TC = false,
+          bool UM = false>
 __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* piv_out,
-                                              int* info_out, int cw, bool fold,
-                                              unsigned char* smem_raw)
+                                              int* info_out, int cw, bool fold_arg,
+                                              unsigned char* smem_raw, UmCtx* um = nullptr)
 {
+    static_assert(!UM || (sizeof(T) == 4 && TC && PIVOT && JB % 8 == 0), "tcgen05 variant");
+    const bool fold = UM ? false : fold_arg;
     static_assert(JB % 4 == 0 && JB <= 32, "panel width");
     static_assert(NT % 32 == 0 && NT <= 1024, "CTA size");
     using K = typename KeyOf<T>::type;
@@ -666,7 +825,8 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             }
             __syncthreads();
             // A22 -= L21 U12: 32x32 tiles of (mt x ncol); L21 rows through the slot table
-            const int tm = (mt + 31) / 32, tn = ncp / 32;
+            // (the UM variant updates A22 after the chunk loop, on tcgen05)
+            const int tm = UM ? 0 : (mt + 31) / 32, tn = ncp / 32;
             for(int t = warp; t < tm * tn; t += NW)
             {
                 const int r0 = (t % tm) * 32, cc0 = (t / tm) * 32;
@@ -703,7 +863,13 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                 __syncthreads();
             }
         }
+        if constexpr(UM)
+            umma_update<NT, JB>(a, lda, j0, jb, mt, n, reinterpret_cast<const float*>(sP), ldp,
+                                slotof, cw, *um);
     }
+    if constexpr(UM)
+        if(um->failed && tid == 0)
+            inf = INT_MIN; // a tensor-core completion wait ran out: results are not valid
     if(tid == 0)
         *info_out = inf;
 }
@@ -711,10 +877,12 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
 // 128-thread CTAs: 3 per SM, or LU_MIN_BLOCKS_128 when the panel fits the smaller register
 // budget (FP32, or one row per thread); 256-thread CTAs: LU_MIN_BLOCKS, or one per SM for
 // panels of more than 32 registers per thread (two rows of a 32-wide panel)
-template <typename T, int NT, int R, int JB, int TN, bool PIVOT, bool TC = false>
+template <typename T, int NT, int R, int JB, int TN, bool PIVOT, bool TC = false,
+          bool UM = false>
 __global__ void __launch_bounds__(NT,
-                                  NT <= 128 ? ((sizeof(T) == 4 || R == 1) ? LU_MIN_BLOCKS_128 : 3)
-                                            : (R * JB > 32 ? 1 : LU_MIN_BLOCKS))
+                                  UM ? (NT <= 128 ? 2 : 1)
+                                  : NT <= 128 ? ((sizeof(T) == 4 || R == 1) ? LU_MIN_BLOCKS_128 : 3)
+                                              : (R * JB > 32 ? 1 : LU_MIN_BLOCKS))
     getrf_cta_kernel(int m, int n, Batch<T> A, int lda, int* ipiv, int64_t strideP, int* info,
                      int cw, int fold, Gate gate)
 {
@@ -722,9 +890,45 @@ __global__ void __launch_bounds__(NT,
     const int64_t b = blockIdx.x;
     if(gate.skip(b))
         return;
-    getrf_cta_dev<T, NT, R, JB, TN, PIVOT, TC>(m, n, A.at(b), lda,
-                                               PIVOT ? ipiv + b * strideP : nullptr, info + b,
-                                               cw, fold != 0, smem_raw);
+    if constexpr(!UM)
+    {
+        getrf_cta_dev<T, NT, R, JB, TN, PIVOT, TC>(m, n, A.at(b), lda,
+                                                   PIVOT ? ipiv + b * strideP : nullptr,
+                                                   info + b, cw, fold != 0, smem_raw);
+    }
+    else
+    {
+        // tcgen05 buffers after the LU's own shared memory; TMEM for one M-tile group
+        __shared__ UmCtx um;
+        uintptr_t p = reinterpret_cast<uintptr_t>(smem_raw) + CtaLuSmem<T, NT, JB>::bytes(m, cw, R);
+        p = (p + 1023) & ~uintptr_t(1023);
+        const int gmax = um_group_max<NT, JB>();
+        const uint32_t ncols = umma::tmem_cols((uint32_t)(um_group<NT, JB>(cw) * cw));
+        if(threadIdx.x == 0)
+        {
+            um.ahi = reinterpret_cast<float*>(p);
+            um.alo = um.ahi + gmax * 128 * JB;
+            um.bhi = um.alo + gmax * 128 * JB;
+            um.blo = um.bhi + cw * JB;
+            um.mbar = reinterpret_cast<uint64_t*>(um.blo + cw * JB);
+            um.G = um_group<NT, JB>(cw);
+            um.phase = 0;
+            um.failed = 0;
+            umma::mbar_init(um.mbar, 1);
+        }
+        if(threadIdx.x < 32)
+            umma::tmem_alloc(reinterpret_cast<uint32_t*>(&um.tmem), ncols);
+        umma::fence_before_sync();
+        __syncthreads();
+        umma::fence_after_sync();
+        UmCtx mine = um; // per-thread copy: the phase and failure state advance in lockstep
+        getrf_cta_dev<T, NT, R, JB, TN, PIVOT, TC, true>(m, n, A.at(b), lda, ipiv + b * strideP,
+                                                         info + b, cw, false, smem_raw, &mine);
+        umma::fence_before_sync();
+        __syncthreads();
+        if(threadIdx.x < 32)
+            umma::tmem_free(mine.tmem, ncols);
+    }
 }
 
 } // namespace rsb
