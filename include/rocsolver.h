@@ -1143,7 +1143,8 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_vbatched_noalloc(rocblas_handle 
  *   getrf    <s|d|t> <m_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold>
  *   vbatched <s|d> <n_max> <threads> <rows_per_thread> <panel_width> <chunk> <fold> <ctas_per_sm>
  * (t: the FP32 LU with split-TF32 updates of sgetrf_tf32 and dsgesv; without t entries it
- * uses the s entries).  It is written by the autotuner (python -m rocsolver_b200.tune) and read when the first
+ * uses the s entries; fold = 2 in a t entry runs its trailing updates on the tcgen05 tensor
+ * cores).  It is written by the autotuner (python -m rocsolver_b200.tune) and read when the first
  * handle is created, from $ROCSOLVER_B200_TUNING or else tuning_b200.txt beside the
  * library.  Entries that name an unavailable configuration fall back to the built-in
  * choice; results do not depend on the table, only speed does. */

@@ -141,6 +141,38 @@ __device__ __forceinline__ int warp_argmax(uint32_t key, int row, bool valid, ui
     return r;
 }
 
+// warp_argmax with the common case cut short: when a single lane holds the largest key
+// (the high 32 bits of a 64-bit key already decide it almost always) its row comes from that
+// lane by one shuffle; the full tie-breaking reductions run only when keys collide.  Same
+// result as warp_argmax (largest key, smallest row on ties; INT_MAX if no lane is valid).
+__device__ __forceinline__ int warp_argmax_fast(uint64_t key, int row, bool valid)
+{
+    const unsigned full = 0xffffffffu;
+    const uint32_t hi = valid ? (uint32_t)(key >> 32) : 0u;
+    const uint32_t mhi = __reduce_max_sync(full, hi);
+    const unsigned mh = __ballot_sync(full, valid && hi == mhi);
+    if(__popc(mh) == 1)
+        return __shfl_sync(full, row, __ffs(mh) - 1);
+    const bool inhi = valid && hi == mhi;
+    const uint32_t mlo = __reduce_max_sync(full, inhi ? (uint32_t)key : 0u);
+    const bool match = inhi && (uint32_t)key == mlo;
+    const unsigned ml = __ballot_sync(full, match);
+    if(__popc(ml) == 1)
+        return __shfl_sync(full, row, __ffs(ml) - 1);
+    return (int)__reduce_min_sync(full, (unsigned)(match ? row : INT_MAX));
+}
+__device__ __forceinline__ int warp_argmax_fast(uint32_t key, int row, bool valid)
+{
+    const unsigned full = 0xffffffffu;
+    const uint32_t k = valid ? key : 0u;
+    const uint32_t mk = __reduce_max_sync(full, k);
+    const bool match = valid && key == mk;
+    const unsigned mm = __ballot_sync(full, match);
+    if(__popc(mm) == 1)
+        return __shfl_sync(full, row, __ffs(mm) - 1);
+    return (int)__reduce_min_sync(full, (unsigned)(match ? row : INT_MAX));
+}
+
 // LAPACK getf2 column scaling: multiply by the reciprocal when |pivot| >= sfmin,
 // otherwise divide (dgetf2; the reference always multiplies,
 // specialized/roclapack_getf2_specialized_kernels.hpp:96-99, which differs only for

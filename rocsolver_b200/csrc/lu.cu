@@ -4,6 +4,8 @@
 // (library/src/include/ideal_sizes.hpp:208-240 getrf, :166-180 potrf;
 // roclapack_getf2.hpp:181-276 select_spkernel): the CTA LU configuration comes from the
 // run-time tuning table (tuning.h) when it has an entry, else from the built-in choice.
+#include <algorithm>
+
 #include "chol.cuh"
 #include "launch.h"
 #include "logger.h"
@@ -111,6 +113,33 @@ static rocblas_status run_getrf_cta(cudaStream_t s, int m, int n, Batch<T> A, in
     return launch_status();
 }
 
+// two-level FP32 LU (outer panels of 64 columns, tcgen05 trailing updates with K = 64)
+template <int NT, int R, int JB>
+static rocblas_status run_getrf_cta2(cudaStream_t s, int m, int n, Batch<float> A, int lda,
+                                     int* ipiv, int64_t sP, int* info, int bc, Gate g, int cw,
+                                     bool* ran)
+{
+    *ran = false;
+    if(m > NT * R)
+        return rocblas_status_not_implemented;
+    const int nround = ((n + 31) / 32) * 32;
+    if(cw <= 0)
+        cw = 128;
+    cw = ((cw + 31) / 32) * 32;
+    cw = std::min(std::min(cw, 256), std::max(nround, 32));
+    const int cwi = LU2_JO;
+    const size_t smem = CtaLuSmem<float, NT, JB>::bytes(m, cwi, R) + lu2_bytes(cw);
+    if(smem > 227 * 1024)
+        return rocblas_status_not_implemented;
+    auto k = getrf_cta2_kernel<NT, R, JB>;
+    if(!set_smem(k, smem))
+        return rocblas_status_internal_error;
+    *ran = true;
+    RSB_LOG_KERNEL("getrf_cta2_kernel");
+    k<<<bc, NT, smem, s>>>(m, n, A, lda, ipiv, sP, info, cw, cwi, g);
+    return launch_status();
+}
+
 // the compiled CTA variants a tuning entry may name: (threads, rows per thread, panel width)
 template <typename T, bool PIVOT, bool TC>
 static rocblas_status run_getrf_tuned(const LuCfg& c, cudaStream_t s, int m, int n,
@@ -122,6 +151,21 @@ static rocblas_status run_getrf_tuned(const LuCfg& c, cudaStream_t s, int m, int
     // that are multiples of 8)
     if constexpr(sizeof(T) == 4 && TC && PIVOT)
     {
+        // fold = 3: two-level LU (outer panels of 64 columns on tcgen05)
+        if(c.fold == 3)
+        {
+#define RSB_LU2_VARIANT(NT_, R_, JB_)                                                          \
+            if(c.nt == NT_ && c.r == R_ && c.jb == JB_)                                        \
+                return run_getrf_cta2<NT_, R_, JB_>(s, m, n, A, lda, ipiv, sP, info, bc, g, c.cw, \
+                                                    ran);
+            RSB_LU2_VARIANT(256, 2, 32)
+            RSB_LU2_VARIANT(256, 2, 16)
+            RSB_LU2_VARIANT(256, 4, 16)
+            RSB_LU2_VARIANT(256, 4, 8)
+            RSB_LU2_VARIANT(256, 8, 8)
+#undef RSB_LU2_VARIANT
+            return rocblas_status_not_implemented;
+        }
         if(c.fold == 2)
         {
 #define RSB_LU_UM_VARIANT(NT_, R_, JB_)                                                        \

@@ -874,6 +874,241 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
         *info_out = inf;
 }
 
+// ---------------------------------------------------------------------------------------
+// Two-level blocking for large orders (FP32, split TF32 on tcgen05).  Outer panels of JO = 64
+// columns are factored by getrf_cta_dev itself (register panels of JB columns whose trailing
+// updates stay inside the outer panel, which is L2-resident), then the outer panel's row
+// interchanges reach the other columns, U12 = L11^{-1} A12 is formed by forward
+// substitution, and A22 -= L21 U12 runs once per outer panel with K = 64 on tcgen05
+// (umma_update_k64): A22 is streamed once per 64 columns instead of once per JB.
+
+constexpr int LU2_JO = 64; // outer panel width (the K of the tcgen05 trailing update)
+
+// Shared memory of the two-level variant after CtaLuSmem's region: one 128-row M-tile of
+// L21 (hi and lo, K = 64), the U12 chunk (hi and lo), mbarrier.  The forward substitution
+// stages L11 (64 x 65 floats) in the M-tile's space.
+__host__ __device__ inline size_t lu2_bytes(int cw)
+{
+    return 1024 + sizeof(float) * (size_t)(2 * 128 * LU2_JO + 2 * cw * LU2_JO) + 64;
+}
+
+// A22 += L21 U12 with K = kk <= 64 on tcgen05, all operands in global memory (column-major,
+// leading dimension lda): A22 = a[r0 + r, c] for r < mt and cfirst <= c < n, L21(r, k) =
+// a[r0 + r, kc0 + k], U12(k, c) = a[kr0 + k, c].  Same structure as umma_update with one
+// M-tile per MMA group (um.G = 1).  All threads of the CTA call it.
+template <int NT>
+__device__ __noinline__ void umma_update_k64(float* a, int lda, int r0, int kc0, int kr0,
+                                             int kk, int mt, int cfirst, int n, int cw,
+                                             UmCtx& um)
+{
+    constexpr int KK = LU2_JO;
+    constexpr int TILE = 128 * KK;
+    constexpr uint32_t SBO = (KK / 4) * 128;
+    if(mt <= 0 || cfirst >= n || um.failed)
+        return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t ahi = umma::smem_u32(um.ahi), alo = umma::smem_u32(um.alo);
+    const uint32_t bhi = umma::smem_u32(um.bhi), blo = umma::smem_u32(um.blo);
+    const int mtiles = (mt + 127) / 128;
+    for(int t = 0; t < mtiles && !um.failed; ++t)
+    {
+        // this M-tile's L21 rows, negated (A22 -= L21 U12 is accumulated as A22 + (-L21) U12;
+        // rows fastest: coalesced column reads)
+        for(int e = tid; e < 128 * KK; e += NT)
+        {
+            const int rl = e & 127, k = e >> 7, r = t * 128 + rl;
+            const float x = (r < mt && k < kk) ? -a[ix(r0 + r, kc0 + k, lda)] : 0.f;
+            uint32_t h, l;
+            umma::split_tf32(x, h, l);
+            const uint32_t off = umma::kmaj_off(rl, k, KK) >> 2;
+            reinterpret_cast<uint32_t*>(um.ahi)[off] = h;
+            reinterpret_cast<uint32_t*>(um.alo)[off] = l;
+        }
+        for(int c0 = cfirst; c0 < n && !um.failed; c0 += cw)
+        {
+            const int ncol = min(cw, n - c0);
+            const int ncp = (ncol + 31) & ~31;
+            for(int e = tid; e < ncp * KK; e += NT)
+            {
+                const int k = e % KK, col = e / KK;
+                const float x = (k < kk && col < ncol) ? a[ix(kr0 + k, c0 + col, lda)] : 0.f;
+                uint32_t h, l;
+                umma::split_tf32(x, h, l);
+                const uint32_t off = umma::kmaj_off(col, k, KK) >> 2;
+                reinterpret_cast<uint32_t*>(um.bhi)[off] = h;
+                reinterpret_cast<uint32_t*>(um.blo)[off] = l;
+            }
+            umma::fence_async_shared();
+            umma::fence_before_sync();
+            __syncthreads();
+            umma::fence_after_sync();
+            if(tid == 0)
+            {
+                const uint32_t idesc = umma::idesc_tf32(128, ncp);
+#pragma unroll
+                for(int s = 0; s < KK / 8; ++s)
+                {
+                    const uint32_t o = 256u * s;
+                    umma::mma_tf32(um.tmem, umma::sdesc(alo + o, 128, SBO),
+                                   umma::sdesc(bhi + o, 128, SBO), idesc, s > 0 ? 1u : 0u);
+                    umma::mma_tf32(um.tmem, umma::sdesc(ahi + o, 128, SBO),
+                                   umma::sdesc(blo + o, 128, SBO), idesc, 1u);
+                    umma::mma_tf32(um.tmem, umma::sdesc(ahi + o, 128, SBO),
+                                   umma::sdesc(bhi + o, 128, SBO), idesc, 1u);
+                }
+                umma::commit(um.mbar);
+            }
+            // epilogue: thread (warp w, lane) owns A22 row t*128 + 32*(w%4) + lane (its TMEM
+            // lane); warpgroup g takes the 16-column blocks g, g + NWG, ...  The first block's
+            // A22 values are loaded while the MMAs run, each next block's before the current
+            // one is stored.
+            constexpr int NWG = NT / 128;
+            const int wg = warp >> 2;
+            const int row = t * 128 + (warp & 3) * 32 + lane;
+            const bool mine = row < mt;
+            float* dst = a + ix(r0 + (mine ? row : 0), c0, lda);
+            float pre[16];
+#pragma unroll
+            for(int j = 0; j < 16; ++j)
+                pre[j] = (mine && wg * 16 + j < ncol) ? dst[(size_t)(wg * 16 + j) * lda] : 0.f;
+            const bool ok = umma::mbar_wait(um.mbar, um.phase);
+            um.phase ^= 1u;
+            if(__syncthreads_or(ok ? 0 : 1))
+            {
+                um.failed = 1;
+                break;
+            }
+            umma::fence_after_sync();
+            for(int cb = wg * 16; cb < ncp; cb += 16 * NWG)
+            {
+                float v[16];
+                umma::tmem_ld16(um.tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)cb, v);
+                const int cn = cb + 16 * NWG;
+                float nxt[16];
+#pragma unroll
+                for(int j = 0; j < 16; ++j)
+                    nxt[j] = (mine && cn + j < ncol) ? dst[(size_t)(cn + j) * lda] : 0.f;
+                if(mine)
+                {
+#pragma unroll
+                    for(int j = 0; j < 16; ++j)
+                        if(cb + j < ncol)
+                            dst[(size_t)(cb + j) * lda] = pre[j] + v[j];
+                }
+#pragma unroll
+                for(int j = 0; j < 16; ++j)
+                    pre[j] = nxt[j];
+            }
+            umma::fence_before_sync();
+            __syncthreads();
+        }
+    }
+}
+
+// U12 = L11^{-1} A12 in place for the outer panel at (j0, j0) of width jo <= 64 (L11 unit
+// lower, staged in shared memory sl as [i][k] with leading dimension 65): one thread per
+// column, in two halves of 32 rows (top: x = L00^{-1} a_top; bottom: a_bot -= L10 x, then
+// x' = L11^{-1} a_bot), the column held in registers.
+template <int NT>
+__device__ __noinline__ void lu2_trsm(float* a, int lda, int j0, int jo, int n, float* sl)
+{
+    constexpr int LD = LU2_JO + 1;
+    for(int e = threadIdx.x; e < LU2_JO * LU2_JO; e += NT)
+    {
+        const int i = e % LU2_JO, k = e / LU2_JO;
+        sl[i * LD + k] = (i < jo && i > k) ? a[ix(j0 + i, j0 + k, lda)] : 0.f;
+    }
+    __syncthreads();
+    for(int c = j0 + jo + threadIdx.x; c < n; c += NT)
+    {
+        float* col = a + ix(j0, c, lda);
+        float x[32];
+#pragma unroll
+        for(int i = 0; i < 32; ++i)
+            x[i] = i < jo ? col[i] : 0.f;
+#pragma unroll
+        for(int k = 0; k < 32; ++k)
+#pragma unroll
+            for(int i = k + 1; i < 32; ++i)
+                x[i] = fmaf(-sl[i * LD + k], x[k], x[i]);
+#pragma unroll
+        for(int i = 0; i < 32; ++i)
+            if(i < jo)
+                col[i] = x[i];
+        if(jo > 32)
+        {
+            float y[32];
+#pragma unroll
+            for(int i = 0; i < 32; ++i)
+                y[i] = 32 + i < jo ? col[32 + i] : 0.f;
+#pragma unroll
+            for(int k = 0; k < 32; ++k)
+#pragma unroll
+                for(int i = 0; i < 32; ++i)
+                    y[i] = fmaf(-sl[(32 + i) * LD + k], x[k], y[i]);
+#pragma unroll
+            for(int k = 0; k < 32; ++k)
+#pragma unroll
+                for(int i = k + 1; i < 32; ++i)
+                    y[i] = fmaf(-sl[(32 + i) * LD + 32 + k], y[k], y[i]);
+#pragma unroll
+            for(int i = 0; i < 32; ++i)
+                if(32 + i < jo)
+                    col[32 + i] = y[i];
+        }
+    }
+    __syncthreads();
+}
+
+// Two-level LU of one m x n FP32 matrix (PIVOT, split TF32): outer panels of LU2_JO columns
+// factored by getrf_cta_dev (inner panel width JB, chunk cwi), the outer trailing update on
+// tcgen05.  smem_raw: CtaLuSmem<float,NT,JB>::bytes(m, cwi, R) then the buffers of um.
+template <int NT, int R, int JB>
+__device__ __forceinline__ void getrf_cta2_dev(int m, int n, float* a, int lda, int* piv_out,
+                                               int* info_out, int cw, int cwi,
+                                               unsigned char* smem_raw, UmCtx& um,
+                                               int* sinf)
+{
+    const int tid = threadIdx.x;
+    const int mn = min(m, n);
+    int inf = 0;
+    for(int j0 = 0; j0 < mn; j0 += LU2_JO)
+    {
+        const int jo = min(LU2_JO, mn - j0);
+        // 1. the outer panel (rows j0.., its jo columns) with the one-level kernel body
+        getrf_cta_dev<float, NT, R, JB, 8, true, true>(m - j0, jo, a + ix(j0, j0, lda), lda,
+                                                       piv_out + j0, sinf, cwi, true, smem_raw);
+        __syncthreads();
+        if(tid < jo)
+            piv_out[j0 + tid] += j0;
+        if(tid == 0 && inf == 0 && *sinf > 0)
+            inf = *sinf + j0;
+        __syncthreads();
+        // 2. its row interchanges on the columns left and right of it, in LAPACK order
+        for(int i = 0; i < jo; ++i)
+        {
+            const int p = piv_out[j0 + i] - 1, q = j0 + i;
+            if(p != q)
+                for(int c = tid; c < n - jo; c += NT)
+                {
+                    const int col = c < j0 ? c : c + jo;
+                    const float t = a[ix(q, col, lda)];
+                    a[ix(q, col, lda)] = a[ix(p, col, lda)];
+                    a[ix(p, col, lda)] = t;
+                }
+            __syncthreads();
+        }
+        if(j0 + jo >= n)
+            continue;
+        // 3. U12 = L11^{-1} A12 (L11 staged in the space of the tcgen05 A operand)
+        lu2_trsm<NT>(a, lda, j0, jo, n, um.ahi);
+        // 4. A22 -= L21 U12 with K = jo
+        umma_update_k64<NT>(a, lda, j0 + jo, j0, j0, jo, m - j0 - jo, j0 + jo, n, cw, um);
+    }
+    if(tid == 0)
+        *info_out = um.failed ? INT_MIN : inf;
+}
+
 // 128-thread CTAs: 3 per SM, or LU_MIN_BLOCKS_128 when the panel fits the smaller register
 // budget (FP32, or one row per thread); 256-thread CTAs: LU_MIN_BLOCKS, or one per SM for
 // panels of more than 32 registers per thread (two rows of a 32-wide panel)
@@ -929,6 +1164,48 @@ __global__ void __launch_bounds__(NT,
         if(threadIdx.x < 32)
             umma::tmem_free(mine.tmem, ncols);
     }
+}
+
+// Two-level FP32 LU (outer panels of 64 columns, K = 64 trailing updates on tcgen05): one CTA
+// per matrix.  cw = outer update column chunk (<= 256), cwi = chunk of the inner panels.
+template <int NT, int R, int JB>
+__global__ void __launch_bounds__(NT, 1)
+    getrf_cta2_kernel(int m, int n, Batch<float> A, int lda, int* ipiv, int64_t strideP,
+                      int* info, int cw, int cwi, Gate gate)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t b = blockIdx.x;
+    if(gate.skip(b))
+        return;
+    __shared__ UmCtx um;
+    __shared__ int sinf;
+    uintptr_t p = reinterpret_cast<uintptr_t>(smem_raw) + CtaLuSmem<float, NT, JB>::bytes(m, cwi, R);
+    p = (p + 1023) & ~uintptr_t(1023);
+    const uint32_t ncols = umma::tmem_cols((uint32_t)cw);
+    if(threadIdx.x == 0)
+    {
+        um.ahi = reinterpret_cast<float*>(p);
+        um.alo = um.ahi + 128 * LU2_JO;
+        um.bhi = um.alo + 128 * LU2_JO;
+        um.blo = um.bhi + cw * LU2_JO;
+        um.mbar = reinterpret_cast<uint64_t*>(um.blo + cw * LU2_JO);
+        um.G = 1;
+        um.phase = 0;
+        um.failed = 0;
+        umma::mbar_init(um.mbar, 1);
+    }
+    if(threadIdx.x < 32)
+        umma::tmem_alloc(reinterpret_cast<uint32_t*>(&um.tmem), ncols);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    UmCtx mine = um;
+    getrf_cta2_dev<NT, R, JB>(m, n, A.at(b), lda, ipiv + b * strideP, info + b, cw, cwi, smem_raw,
+                              mine, &sinf);
+    umma::fence_before_sync();
+    __syncthreads();
+    if(threadIdx.x < 32)
+        umma::tmem_free(mine.tmem, ncols);
 }
 
 } // namespace rsb

@@ -50,13 +50,13 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
         {
             const int buf = k & 1;
             T* row = srow[warp][buf];
+            // every lane forms its candidate's reciprocal while the reduction runs (off the
+            // column's serial path); the winner publishes it
+            const T rc = r[k] != T(0) ? Lim<T>::rcp(r[k]) : T(0);
             int prow = k;
             if(PIVOT)
-            {
-                typename KeyOf<T>::type kk;
-                prow = warp_argmax(pivot_key(r[k], myrow == k), myrow, lane < m && myrow >= k,
-                                   &kk);
-            }
+                prow = warp_argmax_fast(pivot_key(r[k], myrow == k), myrow,
+                                        lane < m && myrow >= k);
             if(myrow == prow)
             {
                 // publish columns from the vector boundary at or below k (the extra leading
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
                         *reinterpret_cast<float4*>(row + j) =
                             make_float4(r[j], r[j + 1], r[j + 2], r[j + 3]);
                 }
-                row[NMAX] = r[k] != T(0) ? Lim<T>::rcp(r[k]) : T(0);
+                row[NMAX] = rc;
             }
             __syncwarp();
             const T piv = row[k];
@@ -90,10 +90,14 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
             }
             if(lane < m && myrow > k)
             {
-                // LAPACK getf2 scaling: reciprocal when |pivot| >= sfmin, else division
-                const int mode = piv == T(0) ? 0 : (fabs(piv) >= Lim<T>::sfmin() ? 1 : 2);
+                // LAPACK getf2 scaling: reciprocal when |pivot| >= sfmin, else division (a
+                // branch uniform across the warp: the division only runs for a subnormal pivot)
                 const T x = r[k];
-                const T l = mode == 1 ? x * rcp : (mode == 2 ? x / piv : x);
+                T l = x;
+                if(fabs(piv) >= Lim<T>::sfmin())
+                    l = x * rcp;
+                else if(piv != T(0))
+                    l = x / piv;
                 r[k] = l;
 #pragma unroll
                 for(int j = 0; j < NMAX; j += VW)

@@ -13,7 +13,9 @@
 // previous entry of the same kind and precision (t = the FP32 LU with split-TF32 trailing
 // updates).  chunk = trailing-update column chunk
 // (multiple of 32; 0 = the default), fold = 1 folds each panel's row interchanges into the
-// trailing update, ctas_per_sm = resident CTAs the persistent kernel launches per SM
+// trailing update, fold = 2 (precision t only) runs the trailing update on the tcgen05
+// tensor cores (operands in shared-memory descriptors, accumulators in TMEM) for the
+// variants compiled with it, ctas_per_sm = resident CTAs the persistent kernel launches per SM
 // (0 = as many as fit).  Entries naming a kernel variant that is not compiled, or one too
 // small for the size, are ignored (the built-in choice applies).
 #pragma once

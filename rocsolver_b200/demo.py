@@ -2,7 +2,9 @@
 
     python -m rocsolver_b200.demo --case getrf --n 256 --batch 512 [--dtype d] [--reps 3]
 
-Cases: getrf, getrs, gesv, potrf, potrs, dsgesv, adjoint, vbatched.  Used to drive
+Cases: getrf, getrs, gesv, potrf, potrs, dsgesv, adjoint, vbatched, sgetrf_tf32 (the FP32
+LU with split-TF32 trailing updates; its kernel configuration, the tcgen05 engine included,
+follows the tuning table, e.g. one named by $ROCSOLVER_B200_TUNING).  Used to drive
 profilers (one small, fixed workload per kernel) and as a usage example of the C ABI from
 Python.  Prints the median device time per call.
 """
@@ -32,7 +34,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
                     choices=["getrf", "getrs", "gesv", "potrf", "potrs", "dsgesv", "adjoint",
-                             "vbatched"])
+                             "vbatched", "sgetrf_tf32"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--nrhs", type=int, default=1)
@@ -41,6 +43,8 @@ def main():
     ap.add_argument("--cond", type=float, default=0.0,
                     help="dsgesv: A = U diag(s) V' with log10(cond) uniform in [1, COND]")
     a = ap.parse_args()
+    if a.case == "sgetrf_tf32":
+        a.dtype = "s"
     dt = torch.float64 if a.dtype == "d" else torch.float32
     dev = torch.device("cuda")
     g = torch.Generator(device=dev)
@@ -87,6 +91,9 @@ def main():
     def call():
         if a.case == "getrf":
             st = rs.call(f"rocsolver_{p}getrf_strided_batched", h.value, n, n, P(A), n, n * n,
+                         P(ipiv), n, P(info), bc)
+        elif a.case == "sgetrf_tf32":
+            st = rs.call("rocsolver_sgetrf_tf32_strided_batched", h.value, n, n, P(A), n, n * n,
                          P(ipiv), n, P(info), bc)
         elif a.case == "getrs":
             st = rs.call(f"rocsolver_{p}getrs_strided_batched", h.value, rs.OP_N, n, nrhs, P(A),

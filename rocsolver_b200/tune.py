@@ -10,7 +10,8 @@ column chunk, and whether the panel's row interchanges are folded into the trail
 update -- on seeded uniform[-1, 1] batches, and keeps the fastest.  For the variable-size
 kernel it also tunes the number of resident CTAs per SM, on batches with n uniform in
 [8, n_max] and nrhs uniform in [1, 16].  Precision t is the FP32 LU with split-TF32
-trailing updates (rocsolver_sgetrf_tf32_strided_batched, the factorisation of dsgesv).
+trailing updates (rocsolver_sgetrf_tf32_strided_batched, the factorisation of dsgesv); its
+candidates include the tcgen05 trailing update (fold = 2) for the variants compiled with it.
 
 The table (format in include/rocsolver.h, rocsolver_b200_tuning_set) is written to
 rocsolver_b200/tuning_b200.txt by default, where the library reads it when the first
@@ -35,6 +36,11 @@ LU_VARIANTS = [(64, 1, 32), (128, 1, 32), (128, 2, 32), (128, 2, 16), (128, 4, 1
                (256, 8, 4), (256, 8, 8)]
 VB_VARIANTS = [(256, 1, 32), (256, 2, 16), (256, 2, 32), (256, 4, 8), (256, 4, 16),
                (256, 8, 4)]
+# variants compiled with the tcgen05 trailing update (precision t, fold = 2) and with the
+# two-level LU (outer panels of 64 columns, K = 64 tcgen05 updates; fold = 3)
+UM_VARIANTS = [(128, 1, 32), (128, 2, 32), (256, 1, 32), (256, 2, 32), (256, 2, 16),
+               (256, 4, 16), (256, 4, 8), (256, 8, 8)]
+LU2_VARIANTS = [(256, 2, 32), (256, 2, 16), (256, 4, 16), (256, 4, 8), (256, 8, 8)]
 # batch per getrf size class (enough CTAs for several waves on 148 SMs)
 GETRF_CLASSES = {64: 16384, 128: 8192, 256: 2048, 512: 592, 1024: 296, 2048: 148}
 VB_CLASSES = {256: 4096, 512: 4096, 1024: 1024}
@@ -53,7 +59,7 @@ def _time(fn, reset, reps):
     return statistics.median(ts[1:])
 
 
-def _lu_candidates(n, quick):
+def _lu_candidates(n, quick, prec="d"):
     out = []
     for nt, r, jb in LU_VARIANTS:
         if nt * r < n or nt * r >= 4 * n:
@@ -61,7 +67,12 @@ def _lu_candidates(n, quick):
         for cw in ((64, 128) if quick else (32, 64, 96, 128)):
             if cw > ((n + 31) // 32) * 32:
                 continue
-            for fold in (0, 1):
+            folds = (0, 1)
+            if prec == "t" and (nt, r, jb) in UM_VARIANTS:
+                folds += (2,)
+            if prec == "t" and (nt, r, jb) in LU2_VARIANTS and n >= 256:
+                folds += (3,)
+            for fold in folds:
                 out.append((nt, r, jb, cw, fold))
     return out
 
@@ -91,7 +102,7 @@ def tune_getrf(prec, n, bc, reps, quick, log):
         t_builtin = _time(call, reset, reps)
         piv_ref = ipiv.clone()
         best = None
-        for cand in _lu_candidates(n, quick):
+        for cand in _lu_candidates(n, quick, prec):
             nt, r, jb, cw, fold = cand
             rs.set_tuning_table(f"getrf {prec} {n} {nt} {r} {jb} {cw} {fold}\n")
             t = _time(call, reset, reps)
@@ -180,6 +191,8 @@ def main():
     ap.add_argument("--precisions", default="d,s,t")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--quick", action="store_true", help="fewer chunk widths")
+    ap.add_argument("--merge", action="store_true",
+                    help="keep the --out file's rows of the precisions not tuned now")
     a = ap.parse_args()
     logf = open(a.log, "a") if a.log else None
 
@@ -210,6 +223,12 @@ def main():
                              + f"    # {t:.3f} / {tb:.3f} ms, batch {VB_CLASSES.get(n, 1024)}")
     finally:
         rs.set_tuning_table(old)
+    if a.merge and os.path.exists(a.out):
+        tuned = set(a.precisions.split(","))
+        with open(a.out) as f:
+            kept = [ln.rstrip("\n") for ln in f
+                    if ln.split()[:1] in (["getrf"], ["vbatched"]) and ln.split()[1] not in tuned]
+        lines = lines[:3] + kept + lines[3:]
     text = "\n".join(lines) + "\n"
     with open(a.out, "w") as f:
         f.write(text)

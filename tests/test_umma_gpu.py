@@ -116,3 +116,71 @@ def test_dsgesv_on_umma_lu(handle, restore_table, n, cfg):
     X = from_colmajor(host(dX), bc, n, 1, n, n)
     for b in range(bc):
         assert solve_backward_error(A[b], X[b], B[b]) <= 1e-13
+
+
+# ---- two-level LU (fold = 3): outer panels of 64 columns factored by the one-level kernel
+# body, one K = 64 tcgen05 trailing update per outer panel
+LU2_VARIANTS = [(256, 2, 32), (256, 2, 16), (256, 4, 16), (256, 4, 8), (256, 8, 8)]
+LU2_CASES = []
+for nt, r, jb in LU2_VARIANTS:
+    cap = nt * r
+    for n in sorted({min(cap, 300), cap, 200, 65}):
+        LU2_CASES.append((nt, r, jb, n, 128 if n >= 128 else 64))
+
+
+@pytest.mark.parametrize("nt,r,jb,n,cw", LU2_CASES)
+def test_forced_two_level_variant(handle, restore_table, nt, r, jb, n, cw):
+    assert rs.set_tuning_table(f"getrf t {n} {nt} {r} {jb} {cw} 3\n") == rs.SUCCESS
+    bc = 2 if n > 1024 else 3
+    A = uniform_general(n, n, bc, seed=7000 + n + jb).astype(np.float32)
+    LU, ipiv, info = sgetrf_tf32(handle, A)
+    _, oipiv, oinfo = oracle_getrf(A)
+    np.testing.assert_array_equal(info, oinfo)
+    for b in range(bc):
+        be = lu_backward_error(A[b].astype(np.float64), LU[b].astype(np.float64), ipiv[b])
+        assert be / (n * eps_of(np.float32)) < 10, (b, be)
+    if n <= 512:
+        assert (ipiv != oipiv).mean() < 0.02
+
+
+@pytest.mark.parametrize("m,n", [(300, 120), (120, 300), (512, 64), (257, 257), (400, 130)])
+def test_two_level_rectangular_and_singular(handle, restore_table, m, n):
+    assert rs.set_tuning_table("getrf t 512 256 2 32 128 3\n") == rs.SUCCESS
+    A = uniform_general(m, n, 3, seed=m * 11 + n).astype(np.float32)
+    A[1][:, min(m, n) // 2 + 3] = 0.0
+    LU, ipiv, info = sgetrf_tf32(handle, A)
+    _, _, oinfo = oracle_getrf(A)
+    np.testing.assert_array_equal(info, oinfo)
+    assert info[1] != 0 and info[0] == 0
+    mn = min(m, n)
+    for b in (0, 2):
+        L = np.tril(LU[b][:, :mn].astype(np.float64), -1) + np.eye(m, mn)
+        U = np.triu(LU[b][:mn, :].astype(np.float64))
+        PA = A[b].astype(np.float64).copy()
+        for k in range(mn):
+            p = ipiv[b][k] - 1
+            if p != k:
+                PA[[k, p]] = PA[[p, k]]
+        err = np.linalg.norm(PA - L @ U) / np.linalg.norm(A[b])
+        assert err / (max(m, n) * eps_of(np.float32)) < 10
+
+
+@pytest.mark.parametrize("n,cfg", [(512, "256 2 32 128"), (1024, "256 4 16 128")])
+def test_dsgesv_on_two_level_lu(handle, restore_table, n, cfg):
+    assert rs.set_tuning_table(f"getrf t {n} {cfg} 3\n") == rs.SUCCESS
+    bc = 4
+    A = cond_graded(n, bc, seed=800 + n, lo=1.0, hi=5.0)
+    B = np.random.default_rng(n + 1).uniform(-1, 1, (bc, n, 1))
+    dA, dB = dev(to_colmajor(A)), dev(to_colmajor(B))
+    dX = dev(np.zeros(bc * n))
+    dP = dev(np.zeros(bc * n, np.int32))
+    dI = dev(np.full(bc, -1, np.int32))
+    dT = dev(np.full(bc, -99, np.int32))
+    st = rs.call("rocsolver_dsgesv_strided_batched", handle, n, 1, ptr(dA), n, n * n, ptr(dP),
+                 n, ptr(dB), n, n, ptr(dX), n, n, ptr(dT), ptr(dI), bc)
+    assert st == rs.SUCCESS
+    it, info = host(dT), host(dI)
+    assert not info.any()
+    X = from_colmajor(host(dX), bc, n, 1, n, n)
+    for b in range(bc):
+        assert solve_backward_error(A[b], X[b], B[b]) <= 1e-13
