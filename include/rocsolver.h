@@ -1154,6 +1154,16 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_b200_tuning_load(const char* path);  /
  * including the NUL. */
 ROCSOLVER_EXPORT size_t rocsolver_b200_tuning_get(char* buf, size_t len);
 
+/* ---- Bounds-checked build (no counterpart in the reference's API; its debug aid is the
+ * ROCSOLVER_VERIFY_ASSUMPTIONS build, library/src/include/lib_host_helpers.hpp:63-80).
+ * librocsolver_b200_checked.so (python -m rocsolver_b200.build --checked) checks every
+ * element access of the factor and solve kernels against the matrix dimensions and every
+ * pivot index against 1..n; a violation is counted and recorded instead of performed.
+ * result[0..3] receives the number of violations since the last call and the first one's
+ * source line and indices, and the record is cleared.  The call synchronises with the
+ * device.  The normal library returns rocblas_status_not_implemented. */
+ROCSOLVER_EXPORT rocblas_status rocsolver_b200_bounds_check(rocblas_int* result);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,7 +17,9 @@ import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 # the in-tree build; $ROCSOLVER_B200_LIB names another build of the same library instead
+# (e.g. the bounds-checked librocsolver_b200_checked.so)
 LIB_PATH = os.environ.get("ROCSOLVER_B200_LIB") or os.path.join(_HERE, "librocsolver_b200.so")
+CHECKED_LIB_PATH = os.path.join(_HERE, "librocsolver_b200_checked.so")
 
 # rocblas_status
 SUCCESS, INVALID_HANDLE, NOT_IMPLEMENTED, INVALID_POINTER, INVALID_SIZE, MEMORY_ERROR, \
@@ -94,6 +96,7 @@ _EXTRA["rocsolver_dgesv_vbatched_noalloc"] = (_c.c_int, [H, P, P, P, P, P, P, P,
 _EXTRA["rocsolver_b200_tuning_set"] = (_c.c_int, [_c.c_char_p])
 _EXTRA["rocsolver_b200_tuning_load"] = (_c.c_int, [_c.c_char_p])
 _EXTRA["rocsolver_b200_tuning_get"] = (_c.c_size_t, [_c.c_char_p, _c.c_size_t])
+_EXTRA["rocsolver_b200_bounds_check"] = (_c.c_int, [_c.c_void_p])
 
 _HANDLE_FUNCS = {
     "rocblas_create_handle": (_c.c_int, [_c.POINTER(H)]),

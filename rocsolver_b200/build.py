@@ -1,9 +1,13 @@
 """Build librocsolver_b200.so in-tree with nvcc for sm_100a.
 
-    python -m rocsolver_b200.build [--force] [--verbose]
+    python -m rocsolver_b200.build [--force] [--verbose] [--checked]
 
 Sources: rocsolver_b200/csrc/*.cu and *.cpp.  Objects go to rocsolver_b200/_build/, the
 shared library to rocsolver_b200/librocsolver_b200.so (loaded by rocsolver_b200/__init__.py).
+--checked builds the bounds-checked variant instead (-DRSB_BOUNDS_CHECK: every element
+access of the factor and solve kernels checked, violations recorded for
+rocsolver_b200_bounds_check) into rocsolver_b200/_build_checked/ and
+rocsolver_b200/librocsolver_b200_checked.so.
 """
 import glob
 import os
@@ -16,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librocsolver_b200.so")
+CHECKED_LIB = os.path.join(HERE, "librocsolver_b200_checked.so")
 ROOT = os.path.dirname(HERE)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -44,17 +49,20 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False):
-    os.makedirs(BUILD, exist_ok=True)
+def build(force=False, verbose=False, checked=False):
+    bdir = BUILD + "_checked" if checked else BUILD
+    lib = CHECKED_LIB if checked else LIB
+    flags = NVCC_FLAGS + (["-DRSB_BOUNDS_CHECK"] if checked else [])
+    os.makedirs(bdir, exist_ok=True)
     srcs = _sources()
     hdrs = _headers() + [os.path.abspath(__file__)]
     objs = []
     jobs = []
     for s in srcs:
-        o = os.path.join(BUILD, os.path.basename(s) + ".o")
+        o = os.path.join(bdir, os.path.basename(s) + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            cmd = [_nvcc()] + ARCH + NVCC_FLAGS + ["-c", s, "-o", o]
+            cmd = [_nvcc()] + ARCH + flags + ["-c", s, "-o", o]
             if verbose and s.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"]
             jobs.append(cmd)
@@ -72,14 +80,15 @@ def build(force=False, verbose=False):
                 failed = True
     if failed:
         raise RuntimeError("nvcc failed")
-    if force or jobs or _stale(LIB, objs):
-        tmp = LIB + ".tmp"
+    if force or jobs or _stale(lib, objs):
+        tmp = lib + ".tmp"
         cmd = [_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart_static", "-lrt",
                                                                    "-lpthread", "-ldl"]
         subprocess.check_call(cmd)
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="--verbose" in sys.argv))
+    print(build(force="--force" in sys.argv, verbose="--verbose" in sys.argv,
+                checked="--checked" in sys.argv))

@@ -62,6 +62,84 @@ __device__ __forceinline__ size_t ix(int i, int j, int ld)
     return (size_t)i + (size_t)j * (size_t)ld;
 }
 
+// ---------------------------------------------------------------------------------------
+// Bounds-checked build (nvcc -DRSB_BOUNDS_CHECK; python -m rocsolver_b200.build --checked).
+// The reference's debug aid is ROCSOLVER_VERIFY_ASSUMPTIONS (library/src/include/
+// lib_host_helpers.hpp:63-80).  Here every element access the factor and solve kernels make
+// through RSB_AT(a, i, j, ld, m, n) checks 0 <= i < m <= ld and 0 <= j < n; a failed check
+// does not trap: it counts the violation, records the first one (source line, i, j) and
+// redirects the access to a scratch element, so the kernel runs to its end and the host
+// reads the record with rocsolver_b200_bounds_check.  RSB_CHECK_PIV(p, n, line) checks a
+// pivot index 1 <= p <= n the same way.  In the normal build both compile to the plain
+// access.
+#ifdef RSB_BOUNDS_CHECK
+namespace bounds {
+struct Record
+{
+    int count, line, i, j;
+};
+static __device__ Record g_rec;        // one per translation unit
+static __device__ double g_scratch[4]; // target of redirected accesses
+__device__ __forceinline__ void fail(int line, int i, int j)
+{
+    if(atomicAdd(&g_rec.count, 1) == 0)
+    {
+        g_rec.line = line;
+        g_rec.i = i;
+        g_rec.j = j;
+    }
+}
+// host side: each translation unit registers a query of its record (bounds.cpp sums them)
+typedef void (*QueryFn)(int* out4);
+void register_query(QueryFn f);
+static void query_tu(int* out4)
+{
+    Record r{};
+    if(cudaMemcpyFromSymbol(&r, g_rec, sizeof(r)) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return;
+    }
+    const Record z{};
+    cudaMemcpyToSymbol(g_rec, &z, sizeof(z));
+    if(r.count && !out4[0])
+    {
+        out4[1] = r.line;
+        out4[2] = r.i;
+        out4[3] = r.j;
+    }
+    out4[0] += r.count;
+}
+static struct Registrar
+{
+    Registrar() { register_query(&query_tu); }
+} g_registrar;
+} // namespace bounds
+template <typename T>
+__device__ __forceinline__ T& at_checked(T* a, int i, int j, int ld, int m, int n, int line)
+{
+    if(i < 0 || i >= m || j < 0 || j >= n || ld < m)
+    {
+        bounds::fail(line, i, j);
+        return *reinterpret_cast<T*>(bounds::g_scratch);
+    }
+    return a[ix(i, j, ld)];
+}
+#define RSB_AT(a, i, j, ld, m, n) (::rsb::at_checked((a), (i), (j), (ld), (m), (n), __LINE__))
+#define RSB_CHECK_PIV(p, n, line)                                                            \
+    do                                                                                       \
+    {                                                                                        \
+        if((p) < 1 || (p) > (n))                                                             \
+            ::rsb::bounds::fail((line), (p), (n));                                           \
+    } while(0)
+#else
+#define RSB_AT(a, i, j, ld, m, n) ((a)[::rsb::ix((i), (j), (ld))])
+#define RSB_CHECK_PIV(p, n, line)                                                            \
+    do                                                                                       \
+    {                                                                                        \
+    } while(0)
+#endif
+
 template <typename T>
 struct Lim;
 template <>

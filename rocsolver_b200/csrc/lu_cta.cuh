@@ -541,7 +541,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             lrow[q] = r;
 #pragma unroll
             for(int c = 0; c < JB; ++c)
-                pv[q][c] = (r < mp && c < jb) ? a[ix(j0 + r, j0 + c, lda)] : T(0);
+                pv[q][c] = (r < mp && c < jb) ? RSB_AT(a, j0 + r, j0 + c, lda, m, n) : T(0);
         }
         // ---------------- factor the panel: rolled column loop, one barrier per column.
         // Warps whose slots all lie below the panel's last row only keep the barrier.
@@ -679,7 +679,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                 for(int k = 0; k < jb; ++k)
                 {
                     const T v = sP[k * ldp + slot];
-                    a[ix(j0 + pos, j0 + k, lda)] = k < pos ? -v : v;
+                    RSB_AT(a, j0 + pos, j0 + k, lda, m, n) = k < pos ? -v : v;
                 }
                 slotof[pos] = slot;
             }
@@ -747,7 +747,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                     {
                         const int i = lane + 32 * s;
                         if(o < nother && i < nm)
-                            v[u][s] = a[ix(j0 + movsrc[i], col, lda)];
+                            v[u][s] = RSB_AT(a, j0 + movsrc[i], col, lda, m, n);
                     }
                 }
                 __syncwarp();
@@ -761,7 +761,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                     {
                         const int i = lane + 32 * s;
                         if(o < nother && i < nm)
-                            a[ix(j0 + moved[i], col, lda)] = v[u][s];
+                            RSB_AT(a, j0 + moved[i], col, lda, m, n) = v[u][s];
                     }
                 }
             }
@@ -793,7 +793,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                 {
                     const int e = e0 + u * NT, k = e % JB, col = e / JB;
                     t[u] = (e < JB * ncp && k < jb && col < ncol)
-                               ? a[ix(j0 + (fold ? slotof[k] : k), c0 + col, lda)]
+                               ? RSB_AT(a, j0 + (fold ? slotof[k] : k), c0 + col, lda, m, n)
                                : T(0);
                 }
 #pragma unroll
@@ -820,7 +820,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                     if(rr < JB)
                         sU[rr * cwp + col] = rr < jb ? v : T(0);
                     if(!fold && rr < jb && col < ncol)
-                        a[ix(j0 + rr, c0 + col, lda)] = v;
+                        RSB_AT(a, j0 + rr, c0 + col, lda, m, n) = v;
                 });
             }
             __syncthreads();
@@ -841,14 +841,14 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                 w.each([&](int rr, int cc, T& v) {
                     const int r = r0 + rr, col = cc0 + cc;
                     v = (r < mt && col < ncol)
-                            ? a[ix(j0 + (fold ? slotof[jb + r] : jb + r), c0 + col, lda)]
+                            ? RSB_AT(a, j0 + (fold ? slotof[jb + r] : jb + r), c0 + col, lda, m, n)
                             : T(0);
                 });
                 w.template mma<JB>(sP, ldp, arow, sU, cwp, cc0);
                 w.each([&](int rr, int cc, T& v) {
                     const int r = r0 + rr, col = cc0 + cc;
                     if(r < mt && col < ncol)
-                        a[ix(j0 + jb + r, c0 + col, lda)] = v;
+                        RSB_AT(a, j0 + jb + r, c0 + col, lda, m, n) = v;
                 });
             }
             __syncthreads();
@@ -858,7 +858,7 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
                 {
                     const int k = e % JB, col = e / JB;
                     if(k < jb)
-                        a[ix(j0 + k, c0 + col, lda)] = sU[k * cwp + col];
+                        RSB_AT(a, j0 + k, c0 + col, lda, m, n) = sU[k * cwp + col];
                 }
                 __syncthreads();
             }

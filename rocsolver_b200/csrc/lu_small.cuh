@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
     T r[NMAX];
 #pragma unroll
     for(int j = 0; j < NMAX; ++j)
-        r[j] = (lane < m && j < n) ? a[ix(lane, j, lda)] : T(0);
+        r[j] = (lane < m && j < n) ? RSB_AT(a, lane, j, lda, m, n) : T(0);
 
     constexpr int VW = 16 / sizeof(T); // elements per 16-byte vector
     int myrow = lane;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
 #pragma unroll
         for(int j = 0; j < NMAX; ++j)
             if(j < n)
-                a[ix(myrow, j, lda)] = r[j];
+                RSB_AT(a, myrow, j, lda, m, n) = r[j];
     }
     if(PIVOT && lane < mn)
         ipiv[b * strideP + lane] = mypiv;
@@ -148,6 +148,8 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
 __device__ __forceinline__ int warp_perm_src(const int* piv, int n, int lane)
 {
     const unsigned full = 0xffffffffu;
+    if(lane < n)
+        RSB_CHECK_PIV(piv[lane], n, __LINE__);
     const int pv = lane < n ? piv[lane] - 1 : lane;
     int x = lane;
     for(int k = n - 1; k >= 0; --k)
@@ -183,7 +185,9 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
     T r[NMAX];
 #pragma unroll
     for(int j = 0; j < NMAX; ++j)
-        r[j] = (lane < n && j < n) ? (trans ? a[ix(j, lane, lda)] : a[ix(lane, j, lda)]) : T(0);
+        r[j] = (lane < n && j < n) ? (trans ? RSB_AT(a, j, lane, lda, n, n)
+                                           : RSB_AT(a, lane, j, lda, n, n))
+                                   : T(0);
     const int src = ipiv ? warp_perm_src(ipiv + b * strideP, n, lane) : lane;
     // reciprocal of this lane's diagonal entry U(lane, lane), computed off the sweeps'
     // serial path (the sweeps multiply by it, as the reference's trsm applies inverted
@@ -198,7 +202,8 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
     T v[NRC];
 #pragma unroll
     for(int c = 0; c < NRC; ++c)
-        v[c] = (lane < n && c0 + c < nrhs) ? x[ix(trans ? lane : src, c0 + c, ldb)] : T(0);
+        v[c] = (lane < n && c0 + c < nrhs) ? RSB_AT(x, trans ? lane : src, c0 + c, ldb, n, nrhs)
+                                           : T(0);
 
     if(!trans)
     {
@@ -274,7 +279,7 @@ __global__ void __launch_bounds__(32 * SMALL_WPB)
 #pragma unroll
     for(int c = 0; c < NRC; ++c)
         if(lane < n && c0 + c < nrhs)
-            x[ix(trans ? src : lane, c0 + c, ldb)] = v[c];
+            RSB_AT(x, trans ? src : lane, c0 + c, ldb, n, nrhs) = v[c];
 }
 
 // Fused gesv for n <= NMAX <= 32 on one warp: factor in registers, then solve with the

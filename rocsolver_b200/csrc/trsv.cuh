@@ -241,7 +241,10 @@ __device__ __forceinline__ void build_perm(const int* piv, int n, int* perm)
     {
         // pivots staged in perm[] (one coalesced load), read back as broadcasts
         for(int k = threadIdx.x; k < n; k += nt)
+        {
+            RSB_CHECK_PIV(piv[k], n, __LINE__);
             perm[k] = piv[k] - 1;
+        }
         __syncthreads();
         const int i0 = threadIdx.x, i1 = threadIdx.x + nt;
         int x0 = i0, x1 = i1;
@@ -361,7 +364,7 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
         n * nc,
         [&](int e) {
             const int i = e % n, c = e / n;
-            return x[ix((!trans && pv) ? perm[i] : i, c0 + c, ldb)];
+            return RSB_AT(x, (!trans && pv) ? perm[i] : i, c0 + c, ldb, n, nrhs);
         },
         [&](int e, T v) { sb[e] = v; });
     __syncthreads();
@@ -379,7 +382,7 @@ __global__ void __launch_bounds__(NT, NT <= 128 ? 1024 / NT : 2)
     {
         const int i = e % n, c = e / n;
         const int dst = (trans && pv) ? perm[i] : i;
-        x[ix(dst, c0 + c, ldb)] = sb[i + c * n];
+        RSB_AT(x, dst, c0 + c, ldb, n, nrhs) = sb[i + c * n];
     }
 }
 
