@@ -39,6 +39,15 @@ typedef int32_t rocblas_int;
 typedef int64_t rocblas_stride;
 typedef struct _rocblas_handle* rocblas_handle;
 typedef uint32_t rocblas_layer_mode_flags;
+/* complex element types, layout-compatible with the reference's (interleaved re, im) */
+typedef struct
+{
+    float x, y;
+} rocblas_float_complex;
+typedef struct
+{
+    double x, y;
+} rocblas_double_complex;
 
 typedef enum rocblas_status_
 {
@@ -598,6 +607,480 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dposv_strided_batched(rocblas_handle h
     const rocblas_int lda,
     const rocblas_stride strideA,
     double* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* ---- complex precisions (c = rocblas_float_complex, z = rocblas_double_complex) --------
+ * The same argument lists as the s / d forms; transposed solves accept
+ * rocblas_operation_conjugate_transpose (op(A) = A^H), Cholesky factors a Hermitian
+ * positive definite matrix (A = L L^H or U^H U). */
+/* replaces rocsolver-functions.h:5155 / lapack/roclapack_getrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetrf(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:5248 / lapack/roclapack_getrf_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetrf_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:5351 / lapack/roclapack_getrf_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetrf_strided_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:4623 / lapack/roclapack_getrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetrf_npvt(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:4703 / lapack/roclapack_getrf_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetrf_npvt_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:4791 / lapack/roclapack_getrf_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetrf_npvt_strided_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8582 / lapack/roclapack_getrs.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetrs(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_int* ipiv,
+    rocblas_float_complex* B,
+    const rocblas_int ldb);
+
+/* replaces rocsolver-functions.h:8681 / lapack/roclapack_getrs_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetrs_batched(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_float_complex* const B[],
+    const rocblas_int ldb,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8796 / lapack/roclapack_getrs_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetrs_strided_batched(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_float_complex* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8892 / lapack/roclapack_gesv.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgesv(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_float_complex* B,
+    const rocblas_int ldb,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:8992 / lapack/roclapack_gesv_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgesv_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_float_complex* const B[],
+    const rocblas_int ldb,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9109 / lapack/roclapack_gesv_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgesv_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_float_complex* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10202 / lapack/roclapack_potrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cpotrf(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:10276 / lapack/roclapack_potrf_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cpotrf_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10358 / lapack/roclapack_potrf_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cpotrf_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10444 / lapack/roclapack_potrs.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cpotrs(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_float_complex* B,
+    const rocblas_int ldb);
+
+/* replaces rocsolver-functions.h:10537 / lapack/roclapack_potrs_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cpotrs_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_float_complex* const B[],
+    const rocblas_int ldb,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10644 / lapack/roclapack_potrs_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cpotrs_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_float_complex* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10738 / lapack/roclapack_posv.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cposv(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_float_complex* B,
+    const rocblas_int ldb,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:10834 / lapack/roclapack_posv_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cposv_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_float_complex* const B[],
+    const rocblas_int ldb,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10944 / lapack/roclapack_posv_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cposv_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_float_complex* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:5163 / lapack/roclapack_getrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetrf(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:5258 / lapack/roclapack_getrf_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetrf_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:5362 / lapack/roclapack_getrf_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetrf_strided_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:4630 / lapack/roclapack_getrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetrf_npvt(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:4711 / lapack/roclapack_getrf_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetrf_npvt_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:4800 / lapack/roclapack_getrf_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetrf_npvt_strided_batched(rocblas_handle handle,
+    const rocblas_int m,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8592 / lapack/roclapack_getrs.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetrs(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_int* ipiv,
+    rocblas_double_complex* B,
+    const rocblas_int ldb);
+
+/* replaces rocsolver-functions.h:8693 / lapack/roclapack_getrs_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetrs_batched(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_double_complex* const B[],
+    const rocblas_int ldb,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8810 / lapack/roclapack_getrs_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetrs_strided_batched(rocblas_handle handle,
+    const rocblas_operation trans,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    const rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_double_complex* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:8902 / lapack/roclapack_gesv.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgesv(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_double_complex* B,
+    const rocblas_int ldb,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9004 / lapack/roclapack_gesv_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgesv_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_double_complex* const B[],
+    const rocblas_int ldb,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9123 / lapack/roclapack_gesv_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgesv_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_double_complex* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10209 / lapack/roclapack_potrf.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zpotrf(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:10284 / lapack/roclapack_potrf_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zpotrf_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10367 / lapack/roclapack_potrf_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zpotrf_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10453 / lapack/roclapack_potrs.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zpotrs(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_double_complex* B,
+    const rocblas_int ldb);
+
+/* replaces rocsolver-functions.h:10547 / lapack/roclapack_potrs_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zpotrs_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_double_complex* const B[],
+    const rocblas_int ldb,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10656 / lapack/roclapack_potrs_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zpotrs_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_double_complex* B,
+    const rocblas_int ldb,
+    const rocblas_stride strideB,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10748 / lapack/roclapack_posv.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zposv(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_double_complex* B,
+    const rocblas_int ldb,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:10845 / lapack/roclapack_posv_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zposv_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_double_complex* const B[],
+    const rocblas_int ldb,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:10957 / lapack/roclapack_posv_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zposv_strided_batched(rocblas_handle handle,
+    const rocblas_fill uplo,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_double_complex* B,
     const rocblas_int ldb,
     const rocblas_stride strideB,
     rocblas_int* info,

@@ -93,6 +93,49 @@ def getri(n, A, lda, strideA, ipiv, strideP, info, bc, pivot=True, nthreads=1):
                        _ptr(ipiv), strideP, None, 0, 0, _ptr(info), bc, nthreads)
 
 
+# ---- complex (c/z): complex64 / complex128 numpy buffers; op 0 getrf, 1 getrs (trans 0 N,
+# 1 T, 2 C), 2 potrf, 3 potrs, 4 gesv, 5 posv (oracle/oracle_complex.c)
+def _cbatch(op, A, m=0, n=0, nrhs=0, trans=0, upper=0, pivot=1, lda=1, sA=0, ipiv=None, sP=0,
+            B=None, ldb=1, sB=0, info=None, bc=1):
+    l = lib()
+    if A.dtype == np.complex128:
+        f = l.oracle_zbatch
+    elif A.dtype == np.complex64:
+        f = l.oracle_cbatch
+    else:
+        raise TypeError(A.dtype)
+    f.restype = None
+    f.argtypes = [ctypes.c_int] * 7 + [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
+                                       ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                       ctypes.c_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int]
+    f(op, m, n, nrhs, trans, upper, pivot, _ptr(A), lda, sA, _ptr(ipiv), sP, _ptr(B), ldb, sB,
+      _ptr(info), bc)
+
+
+def cgetrf(m, n, A, lda, strideA, ipiv, strideP, info, bc, pivot=True):
+    _cbatch(0, A, m, n, 0, 0, 0, int(pivot), lda, strideA, ipiv, strideP, None, 1, 0, info, bc)
+
+
+def cgetrs(trans, n, nrhs, A, lda, strideA, ipiv, strideP, B, ldb, strideB, bc):
+    _cbatch(1, A, n, n, nrhs, trans, 0, 1, lda, strideA, ipiv, strideP, B, ldb, strideB, None, bc)
+
+
+def cpotrf(upper, n, A, lda, strideA, info, bc):
+    _cbatch(2, A, n, n, 0, 0, int(upper), 0, lda, strideA, None, 0, None, 1, 0, info, bc)
+
+
+def cpotrs(upper, n, nrhs, A, lda, strideA, B, ldb, strideB, bc):
+    _cbatch(3, A, n, n, nrhs, 0, int(upper), 0, lda, strideA, None, 0, B, ldb, strideB, None, bc)
+
+
+def cgesv(n, nrhs, A, lda, strideA, ipiv, strideP, B, ldb, strideB, info, bc):
+    _cbatch(4, A, n, n, nrhs, 0, 0, 1, lda, strideA, ipiv, strideP, B, ldb, strideB, info, bc)
+
+
+def cposv(upper, n, nrhs, A, lda, strideA, B, ldb, strideB, info, bc):
+    _cbatch(5, A, n, n, nrhs, 0, int(upper), 0, lda, strideA, None, 0, B, ldb, strideB, info, bc)
+
+
 def refgen(count):
     """Reference client's integer stream (mt19937(69069), uniform_int 1..10)."""
     out = np.empty(count, dtype=np.float64)

@@ -20,7 +20,7 @@ LIB = os.path.join(OUT_DIR, "liboracle.so")
 
 def build(force: bool = False) -> str:
     srcs = [os.path.join(HERE, "oracle.c"), os.path.join(HERE, "refgen.cpp"),
-            os.path.join(HERE, "lapack_host.c")]
+            os.path.join(HERE, "lapack_host.c"), os.path.join(HERE, "oracle_complex.c")]
     if not force and os.path.exists(LIB):
         lib_t = os.path.getmtime(LIB)
         if all(os.path.getmtime(s) <= lib_t for s in srcs + [__file__]):
@@ -29,6 +29,7 @@ def build(force: bool = False) -> str:
     obj_c = os.path.join(OUT_DIR, "oracle.o")
     obj_cpp = os.path.join(OUT_DIR, "refgen.o")
     obj_lh = os.path.join(OUT_DIR, "lapack_host.o")
+    obj_cx = os.path.join(OUT_DIR, "oracle_complex.o")
     # -ffp-contract=off: the restatement must round like the unfused reference BLAS loops
     subprocess.check_call(["gcc", "-O2", "-fPIC", "-ffp-contract=off", "-std=c11", "-Wall",
                            "-c", srcs[0], "-o", obj_c])
@@ -36,8 +37,10 @@ def build(force: bool = False) -> str:
                            "-o", obj_cpp])
     subprocess.check_call(["gcc", "-O2", "-fPIC", "-std=c11", "-Wall", "-c", srcs[2],
                            "-o", obj_lh])
+    subprocess.check_call(["gcc", "-O2", "-fPIC", "-ffp-contract=off", "-std=c11", "-Wall",
+                           "-c", srcs[3], "-o", obj_cx])
     tmp = LIB + ".tmp"
-    subprocess.check_call(["g++", "-shared", "-o", tmp, obj_c, obj_cpp, obj_lh, "-lm",
+    subprocess.check_call(["g++", "-shared", "-o", tmp, obj_c, obj_cpp, obj_lh, obj_cx, "-lm",
                            "-lpthread", "-ldl"])
     os.replace(tmp, LIB)
     return LIB

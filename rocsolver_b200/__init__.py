@@ -78,6 +78,10 @@ _SIG = {
     "gesv_outofplace": [I, I, P, I, P, P, I, P, I, P],
 }
 
+# families the complex precisions (c, z) export: the factor-and-solve ones
+_COMPLEX_FAMILIES = [f for f in _SIG if f.startswith(("getrf", "getrs", "gesv", "potr", "posv"))
+                     and f != "gesv_outofplace"]
+
 # entry points with no counterpart in the reference (declared in include/rocsolver.h)
 _EXTRA = {
     "rocsolver_dsgesv_strided_batched": (_c.c_int, [H, I, I, P, I, S, P, S, P, I, S, P, I, S, P,
@@ -128,6 +132,7 @@ def entry_points():
     """Every exported entry point name (reference ones first, then the handle shim and
     the new ones)."""
     names = [f"rocsolver_{p}{f}" for p in "sd" for f in _SIG]
+    names += [f"rocsolver_{p}{f}" for p in "cz" for f in _COMPLEX_FAMILIES]
     names += list(_HANDLE_FUNCS) + list(_EXTRA)
     return names
 
@@ -141,8 +146,10 @@ def lib():
     if not os.path.exists(LIB_PATH):
         raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m rocsolver_b200.build`")
     l = _c.CDLL(LIB_PATH)
-    for p in "sd":
+    for p in "sdcz":
         for fam, args in _SIG.items():
+            if p in "cz" and fam not in _COMPLEX_FAMILIES:
+                continue
             f = getattr(l, f"rocsolver_{p}{fam}")
             f.restype = _c.c_int
             f.argtypes = [H] + args

@@ -32,6 +32,22 @@ inline bool bad_fill(rocblas_fill f)
 }
 
 template <typename T>
+struct is_complex
+{
+    static constexpr bool value = false;
+};
+template <>
+struct is_complex<rocblas_float_complex>
+{
+    static constexpr bool value = true;
+};
+template <>
+struct is_complex<rocblas_double_complex>
+{
+    static constexpr bool value = true;
+};
+
+template <typename T>
 rocblas_status getrf_impl(rocblas_handle h, int m, int n, Batch<T> A, const void* Aptr, int lda,
                           int* ipiv, int64_t strideP, int* info, int bc, bool pivot,
                           bool tc = false)
@@ -74,8 +90,11 @@ rocblas_status getrs_impl(rocblas_handle h, rocblas_operation trans, int n, int 
         return rocblas_status_success;
     RSB_LOG_STEP("getrs", logging::arg("trans", trans), logging::arg("n", n), logging::arg("nrhs", nrhs),
                  logging::arg("lda", lda), logging::arg("ldb", ldb), logging::arg("bc", bc));
-    return launch_getrs<T>(h->stream, trans == rocblas_operation_none ? 0 : 1, n, nrhs, A, lda,
-                           ipiv, strideP, B, ldb, nullptr, bc);
+    // 0 = N, 1 = T, 2 = C; for the real types C is T
+    const int t = trans == rocblas_operation_none        ? 0
+                  : trans == rocblas_operation_transpose || !is_complex<T>::value ? 1
+                                                                                  : 2;
+    return launch_getrs<T>(h->stream, t, n, nrhs, A, lda, ipiv, strideP, B, ldb, nullptr, bc);
 }
 
 template <typename T>
@@ -720,6 +739,8 @@ extern "C" rocblas_status rocsolver_sgetrf_tf32_strided_batched(
 extern "C" {
 RSB_API_TYPE(s, float)
 RSB_API_TYPE(d, double)
+RSB_API_TYPE(c, rocblas_float_complex)
+RSB_API_TYPE(z, rocblas_double_complex)
 RSB_API_GETRI(s, float)
 RSB_API_GETRI(d, double)
 }

@@ -32,6 +32,26 @@ rocblas_status launch_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T>
                             Batch<T> B, int ldb, const int* skip_info, int bc);
 rocblas_status launch_reset_info(cudaStream_t s, int* info, int bc);
 
+// the complex precisions (complex.cu); getrs takes trans 2 = conjugate transpose
+#define RSB_DECLARE_COMPLEX_LAUNCHERS(C)                                                      \
+    template <>                                                                               \
+    rocblas_status launch_getrf<C>(cudaStream_t, int, int, Batch<C>, int, int*, int64_t, int*,\
+                                   int, bool, Gate, bool);                                    \
+    template <>                                                                               \
+    rocblas_status launch_getrs<C>(cudaStream_t, int, int, int, Batch<C>, int, const int*,    \
+                                   int64_t, Batch<C>, int, const int*, int, Gate);            \
+    template <>                                                                               \
+    rocblas_status launch_gesv<C>(cudaStream_t, int, int, Batch<C>, int, int*, int64_t,       \
+                                  Batch<C>, int, int*, int);                                  \
+    template <>                                                                               \
+    rocblas_status launch_potrf<C>(cudaStream_t, int, int, Batch<C>, int, int*, int);         \
+    template <>                                                                               \
+    rocblas_status launch_potrs<C>(cudaStream_t, int, int, int, Batch<C>, int, Batch<C>, int, \
+                                   const int*, int);
+RSB_DECLARE_COMPLEX_LAUNCHERS(rocblas_float_complex)
+RSB_DECLARE_COMPLEX_LAUNCHERS(rocblas_double_complex)
+#undef RSB_DECLARE_COMPLEX_LAUNCHERS
+
 // inverse from the LU factors (getri.cu): C.base == C.ptrs == nullptr means in place (the
 // inverse is formed in ws, getri_workspace bytes, and copied over A where info == 0);
 // ipiv == nullptr means no pivoting (npvt forms)

@@ -26,7 +26,13 @@ bundled with scipy (scipy.linalg.lapack).  This script runs it on
     nrhs = 4 solve at n = 256;
 
 and stores the LAPACK outputs in lapack_golden.npz (the inputs are regenerated
-from the same seeded generators in tests/refcases.py).  Run it with
+from the same seeded generators in tests/refcases.py).
+
+The complex precisions go to lapack_golden_complex.npz: LAPACK zgetrf / zgetrs (N, T, C) /
+zpotrf / zpotrs / zgesv (and the c routines on a subset) on the reference's complex test
+inputs (each element two draws of the integer stream, real part first) at a subset of the
+same suite sizes, on complex uniform matrices and on Hermitian positive definite Gram
+matrices.  Run it with
 ``python tests/golden/make_golden.py`` from the repository root.
 """
 import os
@@ -40,7 +46,8 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from tests.refcases import (ref_getrf_input, ref_getrs_input, ref_potrf_input,  # noqa: E402
                             ref_gesv_input, uniform_general, spd_gram, cond_graded,
-                            projections, ref_getri_matrix, ref_getri_singular)
+                            projections, ref_getri_matrix, ref_getri_singular,
+                            uniform_complex, hpd_gram)
 
 BC = 3  # batched variants of the reference suites use batch_count = 3
 
@@ -205,5 +212,85 @@ def main():
     print(path, len(cases), "cases", os.path.getsize(path) // 1024, "KiB")
 
 
+def main_complex():
+    out = {}
+    cases = []
+    for P, cdt in (("z", np.complex128), ("c", np.complex64)):
+        getrf, getrs = getattr(la, P + "getrf"), getattr(la, P + "getrs")
+        potrf, potrs, gesv = getattr(la, P + "potrf"), getattr(la, P + "potrs"), getattr(la, P + "gesv")
+        full = P == "z"
+
+        def lu_of(A):
+            lu, piv, info = getrf(A.astype(cdt), overwrite_a=0)
+            return lu, (piv + 1).astype(np.int32), int(info)
+
+        def put(key, **arrs):
+            for k, v in arrs.items():
+                out[key + "_" + k] = v
+            cases.append(key)
+
+        for m, n in (((32, 16), (50, 40), (70, 100)) if full else ((50, 40),)):
+            for singular in (False, True):
+                A = ref_getrf_input(m, n, m, BC, singular, cplx=True)
+                r = [lu_of(A[b]) for b in range(BC)]
+                put(f"{P}getrf_ref_m{m}_n{n}_s{int(singular)}", LU=np.stack([x[0] for x in r]),
+                    ipiv=np.stack([x[1] for x in r]), info=np.array([x[2] for x in r], np.int32))
+        for n in ((1, 2, 31, 33, 65) if full else (33, 65)):
+            A = uniform_complex(n, n, 4, seed=400 + n)
+            r = [lu_of(A[b]) for b in range(4)]
+            put(f"{P}getrf_uni_n{n}", LU=np.stack([x[0] for x in r]),
+                ipiv=np.stack([x[1] for x in r]), info=np.array([x[2] for x in r], np.int32))
+        for n, nrhs in (((20, 10), (50, 30)) if full else ((20, 10),)):
+            A, B = ref_getrs_input(n, nrhs, BC, cplx=True)
+            r = [lu_of(A[b]) for b in range(BC)]
+            out[f"{P}getrs_ref_n{n}_r{nrhs}_LU"] = np.stack([x[0] for x in r])
+            out[f"{P}getrs_ref_n{n}_r{nrhs}_ipiv"] = np.stack([x[1] for x in r])
+            for trans in (0, 1, 2):
+                xs = []
+                for b in range(BC):
+                    x, info2 = getrs(r[b][0], r[b][1] - 1, B[b].astype(cdt), trans=trans)
+                    assert info2 == 0
+                    xs.append(x)
+                put(f"{P}getrs_ref_n{n}_r{nrhs}_t{trans}", X=np.stack(xs))
+        for n in ((10, 50) if full else (10,)):
+            for lower in (True, False):
+                for singular in (False, True):
+                    A = ref_potrf_input(n, BC, singular, cplx=True)
+                    cs, infos = [], []
+                    for b in range(BC):
+                        c, info = potrf(A[b].astype(cdt), lower=int(lower), clean=0, overwrite_a=0)
+                        cs.append(c); infos.append(int(info))
+                    put(f"{P}potrf_ref_n{n}_L{int(lower)}_s{int(singular)}", C=np.stack(cs),
+                        info=np.array(infos, np.int32))
+        for n in ((1, 33, 64) if full else (33,)):
+            A = hpd_gram(n, 4, seed=500 + n)
+            B = uniform_complex(n, 3, 4, seed=600 + n)
+            for lower in (True, False):
+                cs, xs, infos = [], [], []
+                for b in range(4):
+                    c, info = potrf(A[b].astype(cdt), lower=int(lower), clean=0, overwrite_a=0)
+                    x, info2 = potrs(c, B[b].astype(cdt), lower=int(lower))
+                    cs.append(c); xs.append(x); infos.append(int(info))
+                put(f"{P}potrs_hpd_n{n}_L{int(lower)}", C=np.stack(cs), X=np.stack(xs),
+                    info=np.array(infos, np.int32))
+        for n, nrhs in (((20, 1), (50, 10)) if full else ((20, 1),)):
+            for singular in (False, True):
+                A, B = ref_gesv_input(n, nrhs, BC, singular, cplx=True)
+                pivs, xs, infos = [], [], []
+                for b in range(BC):
+                    lu, piv, x, info = gesv(A[b].astype(cdt), B[b].astype(cdt))
+                    if info != 0:
+                        x = B[b].astype(cdt)
+                    pivs.append((piv + 1).astype(np.int32)); xs.append(x); infos.append(int(info))
+                put(f"{P}gesv_ref_n{n}_r{nrhs}_s{int(singular)}", ipiv=np.stack(pivs),
+                    X=np.stack(xs), info=np.array(infos, np.int32))
+    out["cases"] = np.array(cases)
+    path = os.path.join(HERE, "lapack_golden_complex.npz")
+    np.savez_compressed(path, **out)
+    print(path, len(cases), "cases", os.path.getsize(path) // 1024, "KiB")
+
+
 if __name__ == "__main__":
-    main()
+    if "--complex-only" not in sys.argv:
+        main()
+    main_complex()

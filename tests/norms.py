@@ -10,7 +10,7 @@ def eps_of(dtype):
 
 
 def _lange(kind, M):
-    M = np.abs(np.asarray(M, dtype=np.float64))
+    M = np.abs(np.asarray(M)).astype(np.float64)  # modulus for complex entries (zlange)
     if M.size == 0:
         return 0.0
     if kind == "F":
@@ -27,8 +27,9 @@ def _lange(kind, M):
 def norm_error(kind, ref, test):
     """||ref - test|| / ||ref|| (norm.hpp:68-90).  Returns 0 for a zero reference
     that is matched exactly."""
-    ref = np.asarray(ref, dtype=np.float64)
-    test = np.asarray(test, dtype=np.float64)
+    wide = np.complex128 if np.iscomplexobj(ref) or np.iscomplexobj(test) else np.float64
+    ref = np.asarray(ref, dtype=wide)
+    test = np.asarray(test, dtype=wide)
     d = _lange(kind, ref - test)
     r = _lange(kind, ref)
     if r == 0.0:

@@ -11,9 +11,15 @@ the integer stream.
 import numpy as np
 
 
-def _refstream(count):
+def _refstream(count, cplx=False):
+    """count values of the reference's integer stream; complex values take two draws each,
+    real part first (clients/rocblascommon/rocblas_random.hpp random_generator for
+    rocblas_float_complex / rocblas_double_complex)."""
     import oracle
-    return oracle.refgen(count)
+    if not cplx:
+        return oracle.refgen(count)
+    v = oracle.refgen(2 * count)
+    return v[0::2] + 1j * v[1::2]
 
 
 def _member_view(flat, bc, ld, ncols):
@@ -21,9 +27,10 @@ def _member_view(flat, bc, ld, ncols):
     return flat.reshape(bc, ncols, ld).transpose(0, 2, 1).copy()
 
 
-def ref_getrf_input(m, n, lda, bc, singular):
-    """clients/include/testing_getf2_getrf.hpp:128-180."""
-    A = _member_view(_refstream(bc * lda * n), bc, lda, n)
+def ref_getrf_input(m, n, lda, bc, singular, cplx=False):
+    """clients/include/testing_getf2_getrf.hpp:128-180 (the +400 / -4 act on the real part
+    of a complex element)."""
+    A = _member_view(_refstream(bc * lda * n, cplx), bc, lda, n)
     for b in range(bc):
         for i in range(m):
             for j in range(n):
@@ -35,10 +42,10 @@ def ref_getrf_input(m, n, lda, bc, singular):
     return A[:, :m, :].copy()
 
 
-def ref_getrs_input(n, nrhs, bc):
+def ref_getrs_input(n, nrhs, bc, cplx=False):
     """clients/include/testing_getrs.hpp:125-160 (A before its host getrf, and B)."""
-    A = _member_view(_refstream(bc * n * n), bc, n, n)
-    B = _member_view(_refstream(bc * n * nrhs), bc, n, nrhs)
+    A = _member_view(_refstream(bc * n * n, cplx), bc, n, n)
+    B = _member_view(_refstream(bc * n * nrhs, cplx), bc, n, nrhs)
     idx = np.arange(n)
     for b in range(bc):
         A[b] -= 4.0
@@ -46,9 +53,9 @@ def ref_getrs_input(n, nrhs, bc):
     return A, B
 
 
-def ref_gesv_input(n, nrhs, bc, singular):
+def ref_gesv_input(n, nrhs, bc, singular, cplx=False):
     """clients/include/testing_gesv.hpp:138-180."""
-    A, B = ref_getrs_input(n, nrhs, bc)
+    A, B = ref_getrs_input(n, nrhs, bc, cplx)
     if singular:
         for b in range(bc):
             if b == bc // 4 or b == bc // 2 or b == bc - 1:
@@ -57,13 +64,13 @@ def ref_gesv_input(n, nrhs, bc, singular):
     return A, B
 
 
-def ref_potrf_input(n, bc, singular):
+def ref_potrf_input(n, bc, singular, cplx=False):
     """clients/include/testing_potf2_potrf.hpp:103-140 (non-symmetric; only the
-    referenced triangle matters)."""
-    A = _member_view(_refstream(bc * n * n), bc, n, n)
+    referenced triangle matters; the diagonal becomes a * conj(a) * 400, real)."""
+    A = _member_view(_refstream(bc * n * n, cplx), bc, n, n)
     idx = np.arange(n)
     for b in range(bc):
-        A[b, idx, idx] = A[b, idx, idx] * A[b, idx, idx] * 400.0
+        A[b, idx, idx] = A[b, idx, idx] * np.conj(A[b, idx, idx]) * 400.0
         if singular and (b == bc // 4 or b == bc // 2 or b == bc - 1):
             for i0 in (n // 4 + b, n // 2 + b, n - 1 + b):
                 A[b, i0 % n, i0 % n] = 0.0
@@ -92,6 +99,19 @@ def ref_getri_singular(b, bc, n):
 
 def uniform_general(m, n, bc, seed, lo=-1.0, hi=1.0):
     return np.random.default_rng(seed).uniform(lo, hi, size=(bc, m, n))
+
+
+def uniform_complex(m, n, bc, seed):
+    """Real and imaginary parts independent uniform[-1, 1]."""
+    r = np.random.default_rng(seed).uniform(-1.0, 1.0, size=(2, bc, m, n))
+    return r[0] + 1j * r[1]
+
+
+def hpd_gram(n, bc, seed):
+    """Hermitian positive definite A = G G^H + n I with G complex Gaussian."""
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((bc, n, n)) + 1j * rng.standard_normal((bc, n, n))
+    return G @ np.conj(G.transpose(0, 2, 1)) + n * np.eye(n)[None]
 
 
 def cond_graded(n, bc, seed, lo=1.0, hi=6.0):

@@ -60,7 +60,7 @@ def handle():
     h.close()
 
 
-@pytest.mark.parametrize("p", ["s", "d"])
+@pytest.mark.parametrize("p", ["s", "d", "c", "z"])
 def test_getrf_bad_args(handle, p):
     f = f"rocsolver_{p}getrf_strided_batched"
     # m, n, A, lda, strideA, ipiv, strideP, info, bc
@@ -93,7 +93,7 @@ def test_getrf_bad_args(handle, p):
         == rs.INVALID_HANDLE
 
 
-@pytest.mark.parametrize("p", ["s", "d"])
+@pytest.mark.parametrize("p", ["s", "d", "c", "z"])
 def test_getrs_bad_args(handle, p):
     f = f"rocsolver_{p}getrs_strided_batched"
     ok = dict(t=rs.OP_N, n=1, r=1, A=FAKE, lda=1, sA=1, ipiv=FAKE, sP=1, B=FAKE, ldb=1, sB=1,
@@ -119,7 +119,7 @@ def test_getrs_bad_args(handle, p):
     assert c(n=0, A=NULL, ipiv=NULL, B=NULL) == rs.SUCCESS
 
 
-@pytest.mark.parametrize("p", ["s", "d"])
+@pytest.mark.parametrize("p", ["s", "d", "c", "z"])
 def test_gesv_bad_args(handle, p):
     f = f"rocsolver_{p}gesv_strided_batched"
     ok = dict(n=1, r=1, A=FAKE, lda=1, sA=1, ipiv=FAKE, sP=1, B=FAKE, ldb=1, sB=1, info=FAKE,
@@ -139,7 +139,7 @@ def test_gesv_bad_args(handle, p):
     assert c(bc=0, info=NULL) == rs.SUCCESS
 
 
-@pytest.mark.parametrize("p", ["s", "d"])
+@pytest.mark.parametrize("p", ["s", "d", "c", "z"])
 def test_potrf_potrs_posv_bad_args(handle, p):
     f = f"rocsolver_{p}potrf_strided_batched"
     assert rs.call(f, None, rs.FILL_LOWER, 1, FAKE, 1, 1, FAKE, 1) == rs.INVALID_HANDLE

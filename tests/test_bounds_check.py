@@ -87,6 +87,26 @@ for n in (1, 3, 17, 31, 32, 33, 63, 65, 100, 129, 257):
     rs.check(rs.call("rocsolver_dpotrf_strided_batched", h.value, rs.FILL_LOWER, n, P(dS), n + 1,
                      (n + 1) * n, P(dJ), 2), "potrf")
     check_clean(("potrf", n))
+    # complex: zgetrf (rectangular, then square) with a padded leading dimension, zgetrs
+    # N / T / C on the square factors, zposv upper
+    Z = (uniform_general(n + 2, n, 2, seed=n) + 1j * uniform_general(n + 2, n, 2, seed=n + 7))
+    dZ = torch.from_numpy(to_colmajor(Z, n + 4)).cuda()
+    dP = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+    dI = torch.zeros(2, dtype=torch.int32, device="cuda")
+    rs.check(rs.call("rocsolver_zgetrf_strided_batched", h.value, n + 2, n, P(dZ), n + 4,
+                     (n + 4) * n, P(dP), n, P(dI), 2), "zgetrf")
+    dZ = torch.from_numpy(to_colmajor(Z[:, :n, :].copy(), n + 4)).cuda()
+    rs.check(rs.call("rocsolver_zgetrf_strided_batched", h.value, n, n, P(dZ), n + 4,
+                     (n + 4) * n, P(dP), n, P(dI), 2), "zgetrf")
+    dZB = torch.from_numpy(to_colmajor(Z[:, :n, :2].copy(), n + 1)).cuda()
+    for op in (rs.OP_N, rs.OP_T, rs.OP_C):
+        rs.check(rs.call("rocsolver_zgetrs_strided_batched", h.value, op, n, 2, P(dZ), n + 4,
+                         (n + 4) * n, P(dP), n, P(dZB), n + 1, (n + 1) * 2, 2), "zgetrs")
+    H = spd_gram(n, 2, seed=n).astype(np.complex128)
+    dH = torch.from_numpy(to_colmajor(H, n + 1)).cuda()
+    rs.check(rs.call("rocsolver_zposv_strided_batched", h.value, rs.FILL_UPPER, n, 2, P(dH), n + 1,
+                     (n + 1) * n, P(dZB), n + 1, (n + 1) * 2, P(dI), 2), "zposv")
+    check_clean(("complex", n))
 h.close()
 print("bounds clean")
 '''

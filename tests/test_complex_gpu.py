@@ -1,0 +1,360 @@
+"""GPU parity tests of the complex precisions (c = rocblas_float_complex, z =
+rocblas_double_complex) through the C ABI: getrf (and npvt), getrs with N / T / C, gesv, potrf
+and potrs (Hermitian, lower and upper), posv, in the plain, pointer-array and strided forms.
+The checker is the complex oracle (tests/test_oracle_complex.py pins it to host LAPACK
+zgetrf / zgetrs / zpotrf / zpotrs / zgesv) and the golden fixtures themselves.  Acceptance
+rules are the reference's (clients/include/testing_getf2_getrf.hpp:233-259: ipiv and info
+exact, factors within min(m,n)*eps in the F-norm; testing_getrs.hpp:219-229 and
+testing_gesv.hpp:229-247: solutions within n*eps in the inf-norm; testing_potf2_potrf.hpp:
+186-210: the referenced triangle within n*eps)."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import rocsolver_b200 as rs
+from tests.gpu_util import GpuHandle, dev, host, ptr, ptr_array
+from tests.norms import eps_of, norm_error, norm_error_lower, norm_error_upper
+from tests.refcases import (from_colmajor, hpd_gram, ref_gesv_input, ref_getrf_input,
+                            ref_getrs_input, ref_potrf_input, to_colmajor, uniform_complex)
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "lapack_golden_complex.npz"))
+DT = {"z": np.complex128, "c": np.complex64}
+OPS = {0: rs.OP_N, 1: rs.OP_T, 2: rs.OP_C}
+
+
+def eps(P):
+    return eps_of(np.float64 if P == "z" else np.float32)
+
+
+@pytest.fixture(scope="module")
+def handle():
+    h = GpuHandle()
+    yield h.value
+    h.close()
+
+
+def _call(name, *args):
+    st = rs.call(name, *args)
+    assert st == rs.SUCCESS, (name, rs.STATUS_NAMES[st])
+
+
+def oracle_getrf(A, pivot=True):
+    bc, m, n = A.shape
+    mn = max(min(m, n), 1)
+    flat = to_colmajor(A)
+    ipiv = np.zeros(bc * mn, np.int32)
+    info = np.zeros(bc, np.int32)
+    oracle.cgetrf(m, n, flat, m, m * n, ipiv, mn, info, bc, pivot)
+    return from_colmajor(flat, bc, m, n, m, m * n), ipiv.reshape(bc, -1)[:, :min(m, n)], info
+
+
+def gpu_getrf(handle, P, A, form="strided", pivot=True, lda=None):
+    bc, m, n = A.shape
+    lda = m if lda is None else lda
+    mn = max(min(m, n), 1)
+    dA = dev(to_colmajor(A, lda))
+    dP = dev(np.full(bc * mn, -7, np.int32))
+    dI = dev(np.full(bc, -7, np.int32))
+    npvt = "" if pivot else "_npvt"
+    if form == "strided":
+        args = [ptr(dA), lda, lda * n] + ([ptr(dP), mn] if pivot else []) + [ptr(dI), bc]
+        _call(f"rocsolver_{P}getrf{npvt}_strided_batched", handle, m, n, *args)
+    elif form == "batched":
+        aA = ptr_array(dA, bc, lda * n)
+        args = [ptr(aA), lda] + ([ptr(dP), mn] if pivot else []) + [ptr(dI), bc]
+        _call(f"rocsolver_{P}getrf{npvt}_batched", handle, m, n, *args)
+    else:
+        assert bc == 1
+        args = [ptr(dA), lda] + ([ptr(dP)] if pivot else []) + [ptr(dI)]
+        _call(f"rocsolver_{P}getrf{npvt}", handle, m, n, *args)
+    LU = from_colmajor(host(dA), bc, m, n, lda, lda * n)
+    return LU, host(dP).reshape(bc, mn)[:, :min(m, n)], host(dI)
+
+
+GETRF_CASES = [("z", 32, 16), ("z", 50, 40), ("z", 70, 100), ("c", 50, 40)]
+
+
+@pytest.mark.parametrize("P,m,n", GETRF_CASES)
+@pytest.mark.parametrize("singular", [False, True])
+def test_getrf_reference_inputs(handle, P, m, n, singular):
+    A = ref_getrf_input(m, n, m, 3, singular, cplx=True).astype(DT[P])
+    LU, ipiv, info = gpu_getrf(handle, P, A)
+    key = f"{P}getrf_ref_m{m}_n{n}_s{int(singular)}"
+    np.testing.assert_array_equal(ipiv, GOLD[key + "_ipiv"])
+    np.testing.assert_array_equal(info, GOLD[key + "_info"])
+    for b in range(3):
+        assert norm_error("F", GOLD[key + "_LU"][b], LU[b]) <= min(m, n) * eps(P)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+@pytest.mark.parametrize("m,n", [(1, 1), (2, 2), (31, 31), (33, 33), (65, 65), (129, 97),
+                                 (97, 129), (300, 300)])
+@pytest.mark.parametrize("form", ["strided", "batched"])
+def test_getrf_uniform_vs_oracle(handle, P, m, n, form):
+    A = uniform_complex(m, n, 3, seed=m * 7 + n).astype(DT[P])
+    LU, ipiv, info = gpu_getrf(handle, P, A, form=form, lda=m + 3)
+    oLU, oipiv, oinfo = oracle_getrf(A)
+    np.testing.assert_array_equal(info, oinfo)
+    if P == "z" or m <= 65:
+        np.testing.assert_array_equal(ipiv, oipiv)
+    else:  # FP32 rounding may flip a near tie in |re| + |im|
+        assert (ipiv != oipiv).mean() < 0.02
+    for b in range(3):
+        if np.array_equal(ipiv[b], oipiv[b]):
+            assert norm_error("F", oLU[b], LU[b]) <= 4 * min(m, n) * eps(P)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+def test_getrf_plain_and_npvt(handle, P):
+    A = uniform_complex(40, 40, 1, seed=11).astype(DT[P])
+    LU, ipiv, info = gpu_getrf(handle, P, A, form="plain")
+    oLU, oipiv, _ = oracle_getrf(A)
+    np.testing.assert_array_equal(ipiv, oipiv)
+    assert norm_error("F", oLU[0], LU[0]) <= 40 * eps(P)
+    # npvt on a diagonally dominant matrix, all three forms
+    D = A + 50 * np.eye(40)[None]
+    D3 = np.concatenate([D, D * (1 + 1j), D * 2j])
+    oLU, _, oinfo = oracle_getrf(D3, pivot=False)
+    for form in ("strided", "batched"):
+        LU, _, info = gpu_getrf(handle, P, D3.astype(DT[P]), form=form, pivot=False)
+        np.testing.assert_array_equal(info, oinfo)
+        for b in range(3):
+            assert norm_error("F", oLU[b], LU[b]) <= 40 * eps(P)
+    LU, _, info = gpu_getrf(handle, P, D.astype(DT[P]), form="plain", pivot=False)
+    assert info[0] == 0 and norm_error("F", oLU[0], LU[0]) <= 40 * eps(P)
+
+
+@pytest.mark.parametrize("P,n,nrhs", [("z", 20, 10), ("z", 50, 30), ("c", 20, 10)])
+@pytest.mark.parametrize("trans", [0, 1, 2])
+@pytest.mark.parametrize("form", ["strided", "batched", "plain"])
+def test_getrs_reference_inputs(handle, P, n, nrhs, trans, form):
+    _, B = ref_getrs_input(n, nrhs, 3, cplx=True)
+    base = f"{P}getrs_ref_n{n}_r{nrhs}"
+    LU = GOLD[base + "_LU"].astype(DT[P])
+    ipiv = GOLD[base + "_ipiv"].astype(np.int32)
+    X0 = GOLD[f"{base}_t{trans}_X"]
+    B = B.astype(DT[P])
+    bc = 1 if form == "plain" else 3
+    ldb = n + 1
+    dA, dB = dev(to_colmajor(LU[:bc])), dev(to_colmajor(B[:bc], ldb))
+    dP = dev(ipiv[:bc].reshape(-1).copy())
+    if form == "strided":
+        _call(f"rocsolver_{P}getrs_strided_batched", handle, OPS[trans], n, nrhs, ptr(dA), n,
+              n * n, ptr(dP), n, ptr(dB), ldb, ldb * nrhs, bc)
+    elif form == "batched":
+        aA, aB = ptr_array(dA, bc, n * n), ptr_array(dB, bc, ldb * nrhs)
+        _call(f"rocsolver_{P}getrs_batched", handle, OPS[trans], n, nrhs, ptr(aA), n, ptr(dP),
+              n, ptr(aB), ldb, bc)
+    else:
+        _call(f"rocsolver_{P}getrs", handle, OPS[trans], n, nrhs, ptr(dA), n, ptr(dP), ptr(dB),
+              ldb)
+    X = from_colmajor(host(dB), bc, n, nrhs, ldb, ldb * nrhs)
+    for b in range(bc):
+        assert norm_error("I", X0[b], X[b]) <= n * eps(P)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+@pytest.mark.parametrize("trans", [0, 1, 2])
+def test_getrs_uniform_vs_oracle(handle, P, trans):
+    n, nrhs = 150, 7
+    A = uniform_complex(n, n, 2, seed=77).astype(DT[P])
+    B = uniform_complex(n, nrhs, 2, seed=78).astype(DT[P])
+    LU, ipiv, _ = oracle_getrf(A)
+    fLU = to_colmajor(LU)
+    fP = ipiv.reshape(-1).copy()
+    oB = to_colmajor(B)
+    oracle.cgetrs(trans, n, nrhs, fLU, n, n * n, fP, n, oB, n, n * nrhs, 2)
+    dA, dB, dP = dev(fLU), dev(to_colmajor(B)), dev(fP)
+    _call(f"rocsolver_{P}getrs_strided_batched", handle, OPS[trans], n, nrhs, ptr(dA), n, n * n,
+          ptr(dP), n, ptr(dB), n, n * nrhs, 2)
+    X = from_colmajor(host(dB), 2, n, nrhs, n, n * nrhs)
+    oX = from_colmajor(oB, 2, n, nrhs, n, n * nrhs)
+    for b in range(2):
+        # residual check as well: op(A) X = B
+        opA = A[b] if trans == 0 else (A[b].T if trans == 1 else np.conj(A[b].T))
+        r = np.abs(opA.astype(np.complex128) @ X[b] - B[b]).max()
+        assert r <= 1e3 * n * eps(P) * np.abs(X[b]).max()
+        assert norm_error("I", oX[b], X[b]) <= 50 * n * eps(P)
+
+
+@pytest.mark.parametrize("P,n,nrhs", [("z", 20, 1), ("z", 50, 10), ("c", 20, 1)])
+@pytest.mark.parametrize("singular", [False, True])
+@pytest.mark.parametrize("form", ["strided", "batched"])
+def test_gesv_reference_inputs(handle, P, n, nrhs, singular, form):
+    A, B = ref_gesv_input(n, nrhs, 3, singular, cplx=True)
+    A, B = A.astype(DT[P]), B.astype(DT[P])
+    key = f"{P}gesv_ref_n{n}_r{nrhs}_s{int(singular)}"
+    dA, dB = dev(to_colmajor(A)), dev(to_colmajor(B))
+    dP = dev(np.zeros(3 * n, np.int32))
+    dI = dev(np.full(3, -1, np.int32))
+    if form == "strided":
+        _call(f"rocsolver_{P}gesv_strided_batched", handle, n, nrhs, ptr(dA), n, n * n, ptr(dP),
+              n, ptr(dB), n, n * nrhs, ptr(dI), 3)
+    else:
+        aA, aB = ptr_array(dA, 3, n * n), ptr_array(dB, 3, n * nrhs)
+        _call(f"rocsolver_{P}gesv_batched", handle, n, nrhs, ptr(aA), n, ptr(dP), n, ptr(aB), n,
+              ptr(dI), 3)
+    X = from_colmajor(host(dB), 3, n, nrhs, n, n * nrhs)
+    info = host(dI)
+    np.testing.assert_array_equal(info, GOLD[key + "_info"])
+    np.testing.assert_array_equal(host(dP).reshape(3, n), GOLD[key + "_ipiv"])
+    for b in range(3):
+        if info[b] == 0:
+            assert norm_error("I", GOLD[key + "_X"][b], X[b]) <= n * eps(P)
+        else:  # B untouched for failed members (roclapack_gesv.hpp:163-176)
+            np.testing.assert_array_equal(X[b], B[b])
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+def test_gesv_plain(handle, P):
+    n, nrhs = 45, 3
+    A = uniform_complex(n, n, 1, seed=3).astype(DT[P])
+    B = uniform_complex(n, nrhs, 1, seed=4).astype(DT[P])
+    oA, oB = to_colmajor(A), to_colmajor(B)
+    oP, oI = np.zeros(n, np.int32), np.zeros(1, np.int32)
+    oracle.cgesv(n, nrhs, oA, n, n * n, oP, n, oB, n, n * nrhs, oI, 1)
+    dA, dB = dev(to_colmajor(A)), dev(to_colmajor(B))
+    dP, dI = dev(np.zeros(n, np.int32)), dev(np.full(1, -1, np.int32))
+    _call(f"rocsolver_{P}gesv", handle, n, nrhs, ptr(dA), n, ptr(dP), ptr(dB), n, ptr(dI))
+    assert host(dI)[0] == 0
+    np.testing.assert_array_equal(host(dP), oP)
+    X = from_colmajor(host(dB), 1, n, nrhs, n, n * nrhs)[0]
+    assert norm_error("I", from_colmajor(oB, 1, n, nrhs, n, n * nrhs)[0], X) <= 20 * n * eps(P)
+
+
+def gpu_potrf(handle, P, A, lower, form="strided", lda=None):
+    bc, n, _ = A.shape
+    lda = n if lda is None else lda
+    dA = dev(to_colmajor(A, lda))
+    dI = dev(np.full(bc, -7, np.int32))
+    uplo = rs.FILL_LOWER if lower else rs.FILL_UPPER
+    if form == "strided":
+        _call(f"rocsolver_{P}potrf_strided_batched", handle, uplo, n, ptr(dA), lda, lda * n,
+              ptr(dI), bc)
+    elif form == "batched":
+        aA = ptr_array(dA, bc, lda * n)
+        _call(f"rocsolver_{P}potrf_batched", handle, uplo, n, ptr(aA), lda, ptr(dI), bc)
+    else:
+        _call(f"rocsolver_{P}potrf", handle, uplo, n, ptr(dA), lda, ptr(dI))
+    return from_colmajor(host(dA), bc, n, n, lda, lda * n), host(dI), dA
+
+
+@pytest.mark.parametrize("P,n", [("z", 10), ("z", 50), ("c", 10)])
+@pytest.mark.parametrize("lower", [True, False])
+@pytest.mark.parametrize("singular", [False, True])
+@pytest.mark.parametrize("form", ["strided", "batched"])
+def test_potrf_reference_inputs(handle, P, n, lower, singular, form):
+    A = ref_potrf_input(n, 3, singular, cplx=True).astype(DT[P])
+    C, info, _ = gpu_potrf(handle, P, A, lower, form, lda=n + 2)
+    key = f"{P}potrf_ref_n{n}_L{int(lower)}_s{int(singular)}"
+    np.testing.assert_array_equal(info, GOLD[key + "_info"])
+    f = norm_error_lower if lower else norm_error_upper
+    for b in range(3):
+        nn = n if info[b] == 0 else info[b] - 1
+        assert f("F", GOLD[key + "_C"][b][:nn, :nn], C[b][:nn, :nn]) <= n * eps(P)
+        # the other triangle is not referenced
+        other = np.triu(np.ones((n, n), bool), 1) if lower else np.tril(np.ones((n, n), bool), -1)
+        np.testing.assert_array_equal(C[b][other], A[b][other])
+
+
+@pytest.mark.parametrize("P,n", [("z", 1), ("z", 33), ("z", 64), ("c", 33)])
+@pytest.mark.parametrize("lower", [True, False])
+@pytest.mark.parametrize("form", ["strided", "batched", "plain"])
+def test_potrf_potrs_hermitian(handle, P, n, lower, form):
+    A = hpd_gram(n, 4, seed=500 + n).astype(DT[P])
+    B = uniform_complex(n, 3, 4, seed=600 + n).astype(DT[P])
+    key = f"{P}potrs_hpd_n{n}_L{int(lower)}"
+    bc = 1 if form == "plain" else 4
+    C, info, dA = gpu_potrf(handle, P, A[:bc], lower, form)
+    np.testing.assert_array_equal(info, GOLD[key + "_info"][:bc])
+    f = norm_error_lower if lower else norm_error_upper
+    for b in range(bc):
+        assert f("F", GOLD[key + "_C"][b], C[b]) <= n * eps(P)
+    ldb = n + 1
+    dB = dev(to_colmajor(B[:bc], ldb))
+    uplo = rs.FILL_LOWER if lower else rs.FILL_UPPER
+    if form == "strided":
+        _call(f"rocsolver_{P}potrs_strided_batched", handle, uplo, n, 3, ptr(dA), n, n * n,
+              ptr(dB), ldb, ldb * 3, bc)
+    elif form == "batched":
+        aA, aB = ptr_array(dA, bc, n * n), ptr_array(dB, bc, ldb * 3)
+        _call(f"rocsolver_{P}potrs_batched", handle, uplo, n, 3, ptr(aA), n, ptr(aB), ldb, bc)
+    else:
+        _call(f"rocsolver_{P}potrs", handle, uplo, n, 3, ptr(dA), n, ptr(dB), ldb)
+    X = from_colmajor(host(dB), bc, n, 3, ldb, ldb * 3)
+    for b in range(bc):
+        assert norm_error("I", GOLD[key + "_X"][b], X[b]) <= n * eps(P)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+@pytest.mark.parametrize("lower", [True, False])
+@pytest.mark.parametrize("form", ["strided", "batched", "plain"])
+def test_posv(handle, P, lower, form):
+    n, nrhs = 40, 2
+    bc = 1 if form == "plain" else 3
+    A = hpd_gram(n, bc, seed=9).astype(DT[P])
+    if bc == 3:  # member 1 not positive definite: info > 0 and its B untouched
+        A[1][7, 7] = -1.0
+    B = uniform_complex(n, nrhs, bc, seed=10).astype(DT[P])
+    oA, oB = to_colmajor(A), to_colmajor(B)
+    oI = np.zeros(bc, np.int32)
+    oracle.cposv(not lower, n, nrhs, oA, n, n * n, oB, n, n * nrhs, oI, bc)
+    dA, dB = dev(to_colmajor(A)), dev(to_colmajor(B))
+    dI = dev(np.full(bc, -7, np.int32))
+    uplo = rs.FILL_LOWER if lower else rs.FILL_UPPER
+    if form == "strided":
+        _call(f"rocsolver_{P}posv_strided_batched", handle, uplo, n, nrhs, ptr(dA), n, n * n,
+              ptr(dB), n, n * nrhs, ptr(dI), bc)
+    elif form == "batched":
+        aA, aB = ptr_array(dA, bc, n * n), ptr_array(dB, bc, n * nrhs)
+        _call(f"rocsolver_{P}posv_batched", handle, uplo, n, nrhs, ptr(aA), n, ptr(aB), n,
+              ptr(dI), bc)
+    else:
+        _call(f"rocsolver_{P}posv", handle, uplo, n, nrhs, ptr(dA), n, ptr(dB), n, ptr(dI))
+    info = host(dI)
+    np.testing.assert_array_equal(info, oI)
+    X = from_colmajor(host(dB), bc, n, nrhs, n, n * nrhs)
+    oX = from_colmajor(oB, bc, n, nrhs, n, n * nrhs)
+    for b in range(bc):
+        if info[b] == 0:
+            assert norm_error("I", oX[b], X[b]) <= 10 * n * eps(P)
+        else:
+            np.testing.assert_array_equal(X[b], B[b])
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+def test_nan_and_zero_pivots(handle, P):
+    """A NaN in the first candidate row wins the pivot search, one elsewhere never does
+    (LAPACK izamax); an exactly zero column sets info to its order and the factorisation
+    goes on."""
+    n = 24
+    A = uniform_complex(n, n, 3, seed=21).astype(DT[P])
+    A[0][0, 0] = complex(np.nan, 0)
+    A[1][5, 0] = complex(0, np.nan)
+    A[2][:, 9] = 0
+    LU, ipiv, info = gpu_getrf(handle, P, A)
+    oLU, oipiv, oinfo = oracle_getrf(A)
+    np.testing.assert_array_equal(ipiv[:, :1], oipiv[:, :1])
+    np.testing.assert_array_equal(info, oinfo)
+    assert info[2] == 10
+    np.testing.assert_array_equal(ipiv[2], oipiv[2])
+    assert norm_error("F", oLU[2], LU[2]) <= n * eps(P)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+def test_empty_and_quick_returns(handle, P):
+    dI = dev(np.full(2, -7, np.int32))
+    dA = dev(np.zeros(4, DT[P]))
+    _call(f"rocsolver_{P}getrf_strided_batched", handle, 0, 3, ptr(dA), 1, 0, ptr(dI), 1,
+          ptr(dI), 2)
+    np.testing.assert_array_equal(host(dI), [0, 0])
+    dI = dev(np.full(2, -7, np.int32))
+    _call(f"rocsolver_{P}potrf_strided_batched", handle, rs.FILL_LOWER, 0, ptr(dA), 1, 0, ptr(dI),
+          2)
+    np.testing.assert_array_equal(host(dI), [0, 0])
+    _call(f"rocsolver_{P}getrs_strided_batched", handle, rs.OP_C, 0, 1, None, 1, 0, None, 1,
+          None, 1, 0, 2)
