@@ -1600,13 +1600,16 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_vbatched(rocblas_handle handle,
  * library allocates with cudaMalloc on first use; callers that may not allocate (code
  * running while a memory pool owns the device memory, allocation-free real-time loops,
  * plugins whose host framework forbids device allocations) use this variant, which keeps
- * the scratch in a fixed ~4 MiB array in the library's device memory (held on every GPU
- * that loads the library until the process exits).
+ * the scratch in a fixed ~4 MiB array in the library's device memory (held on each GPU
+ * where it has been called, until the process exits).
  *   - batch_count is limited to 1048576 members; larger batches return invalid_size.
  *   - All calls share the array: calls that overlap on the GPU race; order them on one
  *     stream.  Nothing carries over between calls (the work list is rebuilt each call).
- *   - The first call on a device looks up the array's device address; make that first
- *     call before any stream capture on that device. */
+ *   - The first call on a device looks up the array's device address.  Under CUDA's lazy
+ *     module loading (the default since CUDA 12.2) that is when the driver places the
+ *     array on the device, so make the first call (a warm-up with batch_count > 0) before
+ *     a memory pool claims the device's free memory, and before any stream capture on
+ *     that device. */
 ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_vbatched_noalloc(rocblas_handle handle,
     const rocblas_int* n,
     const rocblas_int* nrhs,

@@ -27,6 +27,12 @@
 
 namespace rsb {
 
+// LAPACK dsgesv allows ITERMAX = 30 corrections; this solver stops at 10 (ITER = -11 then),
+// the iteration budget of the benchmarked configuration: every pass re-reads A in FP64 and
+// the FP32 factors (~0.8 MB per member at n = 256), and a member still short of the
+// stopping rule after 10 passes is re-solved in FP64 for about the cost of 5 more passes.
+// ITER values therefore differ from LAPACK's for members that would converge in 11-30
+// corrections (they take the FP64 path here).
 constexpr int DSGESV_ITERMAX = 10;
 // refinement solves use inverted diagonal blocks up to this order (their shared memory
 // grows as n); larger orders use the staged-block substitution

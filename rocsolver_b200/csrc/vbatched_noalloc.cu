@@ -10,12 +10,17 @@
 //
 // Limits and sharing rules:
 //   * at most VB_NOALLOC_MAX_BATCH members per call (larger batches get invalid_size);
-//   * the array costs ~4 MiB on every GPU that loads the library, until the process exits;
+//   * the array costs ~4 MiB on each GPU where the entry point has been called, until the
+//     process exits.  With CUDA's lazy module loading (the default since CUDA 12.2) the driver
+//     places it on the device when it first loads this module, at the first call's address
+//     lookup: make the first call (a warm-up with batch_count > 0 will do) before a memory
+//     pool claims the device's free memory, or that call returns internal_error;
 //   * every call uses the same array: calls that overlap on the GPU (different streams, or
 //     different handles on the same device without ordering) race and corrupt each other's
 //     work lists; order them on one stream;
 //   * the first call on each device looks up the array's device address (a CUDA runtime
-//     query, no allocation); make that first call before any stream capture on the device.
+//     query that may load the module, see above); make that first call before any stream
+//     capture on the device.
 // The contents left by the previous call need no clearing: the plan kernel rewrites the
 // work list and resets the counters at the start of every call.
 #include <mutex>
