@@ -98,20 +98,20 @@ __device__ int cta_argmax(K key, int row, bool valid, K* skey, int* srow)
     return gr;
 }
 
+// LU of one m x n member at a (leading dimension lda: global memory, or the member's copy in
+// shared memory) by the whole CTA; writes ipiv (PIVOT) and returns info.  Per column: the
+// pivot search over the rows (threads over rows, cta_argmax), the interchange over all
+// columns, the scaling of the column below the diagonal, and the rank-1 update of the
+// trailing matrix with warps over columns and lanes over rows (consecutive rows of a column
+// are contiguous: coalesced in global memory, conflict-free rows in shared memory).
 template <typename C, bool PIVOT>
-__global__ void __launch_bounds__(CPX_NT)
-    cgetrf_kernel(int m, int n, Batch<C> A, int lda, int* ipiv, int64_t strideP, int* info,
-                  Gate gate)
+__device__ int cgetrf_dev(int m, int n, C* a, int lda, int* piv,
+                          typename KeyOf<typename CxReal<C>::R>::type* skey, int* srow)
 {
     using R = typename CxReal<C>::R;
     using K = typename KeyOf<R>::type;
-    __shared__ K skey[CPX_NT / 32];
-    __shared__ int srow[CPX_NT / 32];
-    const int64_t b = blockIdx.x;
-    if(gate.skip(b))
-        return;
-    C* a = A.at(b);
-    const int tid = threadIdx.x;
+    constexpr int NW = CPX_NT / 32;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mn = min(m, n);
     int inf = 0;
     for(int j = 0; j < mn; ++j)
@@ -134,38 +134,40 @@ __global__ void __launch_bounds__(CPX_NT)
             }
             p = cta_argmax(bk, br, br != INT_MAX, skey, srow);
             if(tid == 0)
-                ipiv[b * strideP + j] = p + 1;
+                piv[j] = p + 1;
         }
-        const C piv = RSB_AT(a, p, j, lda, m, n);
+        const C pv = RSB_AT(a, p, j, lda, m, n);
         __syncthreads();
-        if(!czero(piv))
+        if(!czero(pv))
         {
             if(p != j)
+            {
                 for(int c = tid; c < n; c += CPX_NT)
                 {
                     const C t = RSB_AT(a, j, c, lda, m, n);
                     RSB_AT(a, j, c, lda, m, n) = RSB_AT(a, p, c, lda, m, n);
                     RSB_AT(a, p, c, lda, m, n) = t;
                 }
-            __syncthreads();
-            const bool rec = hypot(piv.x, piv.y) >= Lim<R>::sfmin();
-            const C r = rec ? cdiv(cx<C>(1, 0), piv) : piv;
+                __syncthreads();
+            }
+            const bool rec = hypot(pv.x, pv.y) >= Lim<R>::sfmin();
+            const C r = rec ? cdiv(cx<C>(1, 0), pv) : pv;
             for(int i = j + 1 + tid; i < m; i += CPX_NT)
             {
                 C& e = RSB_AT(a, i, j, lda, m, n);
-                e = rec ? cmul(e, r) : cdiv(e, piv);
+                e = rec ? cmul(e, r) : cdiv(e, pv);
             }
         }
         else if(inf == 0)
             inf = j + 1;
         __syncthreads();
         // A(j+1:m, j+1:n) -= A(j+1:m, j) A(j, j+1:n)
-        const int rows = m - j - 1, cols = n - j - 1;
-        for(int64_t e = tid; e < (int64_t)rows * cols; e += CPX_NT)
+        for(int c = j + 1 + warp; c < n; c += NW)
         {
-            const int i = j + 1 + (int)(e % rows), c = j + 1 + (int)(e / rows);
             const C u = RSB_AT(a, j, c, lda, m, n);
-            if(!czero(u))
+            if(czero(u))
+                continue;
+            for(int i = j + 1 + lane; i < m; i += 32)
             {
                 C& t = RSB_AT(a, i, c, lda, m, n);
                 t = csub(t, cmul(RSB_AT(a, i, j, lda, m, n), u));
@@ -173,7 +175,55 @@ __global__ void __launch_bounds__(CPX_NT)
         }
         __syncthreads();
     }
-    if(tid == 0)
+    return inf;
+}
+
+template <typename C, bool PIVOT>
+__global__ void __launch_bounds__(CPX_NT)
+    cgetrf_kernel(int m, int n, Batch<C> A, int lda, int* ipiv, int64_t strideP, int* info,
+                  Gate gate)
+{
+    using K = typename KeyOf<typename CxReal<C>::R>::type;
+    __shared__ K skey[CPX_NT / 32];
+    __shared__ int srow[CPX_NT / 32];
+    const int64_t b = blockIdx.x;
+    if(gate.skip(b))
+        return;
+    const int inf = cgetrf_dev<C, PIVOT>(m, n, A.at(b), lda, PIVOT ? ipiv + b * strideP : nullptr,
+                                         skey, srow);
+    if(threadIdx.x == 0)
+        info[b] = inf;
+}
+
+// members of at most CPX_SMEM_MAX bytes are factored in shared memory (one copy in, one out)
+constexpr int CPX_SMEM_MAX = 96 * 1024;
+
+template <typename C, bool PIVOT>
+__global__ void __launch_bounds__(CPX_NT)
+    cgetrf_smem_kernel(int m, int n, Batch<C> A, int lda, int* ipiv, int64_t strideP, int* info,
+                       Gate gate)
+{
+    using K = typename KeyOf<typename CxReal<C>::R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sa = reinterpret_cast<C*>(smem_raw); // m x n, leading dimension m
+    __shared__ K skey[CPX_NT / 32];
+    __shared__ int srow[CPX_NT / 32];
+    constexpr int NW = CPX_NT / 32;
+    const int64_t b = blockIdx.x;
+    if(gate.skip(b))
+        return;
+    C* a = A.at(b);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for(int c = warp; c < n; c += NW)
+        for(int i = lane; i < m; i += 32)
+            sa[i + (size_t)c * m] = RSB_AT(a, i, c, lda, m, n);
+    __syncthreads();
+    const int inf = cgetrf_dev<C, PIVOT>(m, n, sa, m, PIVOT ? ipiv + b * strideP : nullptr, skey,
+                                         srow);
+    for(int c = warp; c < n; c += NW)
+        for(int i = lane; i < m; i += 32)
+            RSB_AT(a, i, c, lda, m, n) = sa[i + (size_t)c * m];
+    if(threadIdx.x == 0)
         info[b] = inf;
 }
 
@@ -269,17 +319,17 @@ __global__ void __launch_bounds__(CPX_NT)
     }
 }
 
-// Hermitian Cholesky, right-looking: A = L L^H (lower) or U^H U (upper); info = first order
-// whose pivot real(a_jj) - sum |l_jk|^2 is <= 0 or NaN (that value is stored in a_jj, then
-// the factorisation stops, as LAPACK zpotf2 does).  The other triangle is not touched.
+// Hermitian Cholesky of one member at a (global memory, or its copy in shared memory),
+// right-looking: A = L L^H (lower) or U^H U (upper); returns info = first order whose pivot
+// real(a_jj) - sum |l_jk|^2 is <= 0 or NaN (that value is stored in a_jj, then the
+// factorisation stops, as LAPACK zpotf2 does).  The other triangle is not touched.  The
+// trailing update runs with warps over columns and lanes over rows.
 template <typename C>
-__global__ void __launch_bounds__(CPX_NT)
-    cpotrf_kernel(int upper, int n, Batch<C> A, int lda, int* info)
+__device__ int cpotrf_dev(int upper, int n, C* a, int lda)
 {
     using R = typename CxReal<C>::R;
-    const int64_t b = blockIdx.x;
-    C* a = A.at(b);
-    const int tid = threadIdx.x;
+    constexpr int NW = CPX_NT / 32;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for(int j = 0; j < n; ++j)
     {
         const R ajj = RSB_AT(a, j, j, lda, n, n).x;
@@ -287,11 +337,9 @@ __global__ void __launch_bounds__(CPX_NT)
         if(ajj <= R(0) || isnan(ajj))
         {
             if(tid == 0)
-            {
                 RSB_AT(a, j, j, lda, n, n) = cx<C>(ajj, 0);
-                info[b] = j + 1;
-            }
-            return;
+            __syncthreads();
+            return j + 1;
         }
         const R d = sqrt(ajj), rd = R(1) / d;
         if(tid == 0)
@@ -302,26 +350,62 @@ __global__ void __launch_bounds__(CPX_NT)
             e = cx<C>(e.x * rd, e.y * rd);
         }
         __syncthreads();
-        // trailing Hermitian update of the referenced triangle
-        const int t = n - j - 1;
-        for(int64_t e = tid; e < (int64_t)t * t; e += CPX_NT)
+        // trailing Hermitian update of the referenced triangle, column k by one warp
+        for(int k = j + 1 + warp; k < n; k += NW)
         {
-            const int i = j + 1 + (int)(e % t), k = j + 1 + (int)(e / t);
-            if(!upper && i >= k) // L(i,k) -= L(i,j) conj(L(k,j))
+            if(!upper) // L(i,k) -= L(i,j) conj(L(k,j)), i >= k
             {
-                C& v = RSB_AT(a, i, k, lda, n, n);
-                v = csub(v, cmul(RSB_AT(a, i, j, lda, n, n), cconj(RSB_AT(a, k, j, lda, n, n))));
+                const C lk = cconj(RSB_AT(a, k, j, lda, n, n));
+                for(int i = k + lane; i < n; i += 32)
+                {
+                    C& v = RSB_AT(a, i, k, lda, n, n);
+                    v = csub(v, cmul(RSB_AT(a, i, j, lda, n, n), lk));
+                }
             }
-            else if(upper && k >= i) // U(i,k) -= conj(U(j,i)) U(j,k)
+            else // U(i,k) -= conj(U(j,i)) U(j,k), j < i <= k
             {
-                C& v = RSB_AT(a, i, k, lda, n, n);
-                v = csub(v, cmul(cconj(RSB_AT(a, j, i, lda, n, n)), RSB_AT(a, j, k, lda, n, n)));
+                const C uk = RSB_AT(a, j, k, lda, n, n);
+                for(int i = j + 1 + lane; i <= k; i += 32)
+                {
+                    C& v = RSB_AT(a, i, k, lda, n, n);
+                    v = csub(v, cmul(cconj(RSB_AT(a, j, i, lda, n, n)), uk));
+                }
             }
         }
         __syncthreads();
     }
-    if(tid == 0)
-        info[b] = 0;
+    return 0;
+}
+
+template <typename C>
+__global__ void __launch_bounds__(CPX_NT)
+    cpotrf_kernel(int upper, int n, Batch<C> A, int lda, int* info)
+{
+    const int inf = cpotrf_dev<C>(upper, n, A.at(blockIdx.x), lda);
+    if(threadIdx.x == 0)
+        info[blockIdx.x] = inf;
+}
+
+// members of at most CPX_SMEM_MAX bytes: the referenced triangle is factored in shared memory
+template <typename C>
+__global__ void __launch_bounds__(CPX_NT)
+    cpotrf_smem_kernel(int upper, int n, Batch<C> A, int lda, int* info)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sa = reinterpret_cast<C*>(smem_raw); // n x n, leading dimension n
+    constexpr int NW = CPX_NT / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    C* a = A.at(blockIdx.x);
+    for(int c = warp; c < n; c += NW)
+        for(int i = upper ? lane : c + lane; i < (upper ? c + 1 : n); i += 32)
+            sa[i + (size_t)c * n] = RSB_AT(a, i, c, lda, n, n);
+    __syncthreads();
+    const int inf = cpotrf_dev<C>(upper, n, sa, n);
+    for(int c = warp; c < n; c += NW)
+        for(int i = upper ? lane : c + lane; i < (upper ? c + 1 : n); i += 32)
+            RSB_AT(a, i, c, lda, n, n) = sa[i + (size_t)c * n];
+    if(threadIdx.x == 0)
+        info[blockIdx.x] = inf;
 }
 
 // B <- A^{-1} B with the Cholesky factor: lower L Y = B, L^H X = Y; upper U^H Y = B, U X = Y.
@@ -370,6 +454,208 @@ __global__ void __launch_bounds__(CPX_NT)
     }
 }
 
+// ---- warp-per-right-hand-side solves (n <= 32 * Q): lane l holds rows l, l + 32, ... of
+// the vector in registers; no block barriers.  Two sweep forms, chosen so that the lanes read
+// contiguous memory: AXPY (column-oriented: once x_k is final, the rows on the far side of k
+// take T(i,k) x_k, lanes over i) and DOT (row-oriented: x_i = (x_i - sum_k T(i,k) x_k) /
+// T(i,i), lanes over k, one warp reduction per row).  get(i, k) returns the element T(i, k)
+// of the triangular matrix (conjugated by the caller when the solve needs it); FWD solves
+// rows in increasing order (T lower), else decreasing (T upper); UNIT skips the diagonal.
+template <typename C>
+__device__ __forceinline__ C cshfl(C v, int src)
+{
+    return cx<C>(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+template <typename C>
+__device__ __forceinline__ C cshfl_xor(C v, int m)
+{
+    return cx<C>(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+template <typename C, int Q, bool FWD, bool AXPY, bool UNIT, typename Get>
+__device__ __forceinline__ void warp_trsv(int n, C (&x)[Q], Get get)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for(int qs = 0; qs < Q; ++qs)
+    {
+        const int q0 = FWD ? qs : Q - 1 - qs; // register holding the sequential index
+        for(int ks = 0; ks < 32; ++ks)
+        {
+            const int kk = FWD ? ks : 31 - ks;
+            const int k = 32 * q0 + kk; // the row (DOT) or column (AXPY) being finished
+            if(k >= n)
+            {
+                if(FWD)
+                    break;
+                continue;
+            }
+            if(AXPY)
+            {
+                if(!UNIT && lane == kk)
+                    x[q0] = cdiv(x[q0], get(k, k));
+                const C xk = cshfl(x[q0], kk);
+#pragma unroll
+                for(int q = 0; q < Q; ++q)
+                {
+                    const int i = lane + 32 * q;
+                    if((FWD ? q >= q0 : q <= q0) && (FWD ? i > k : i < k) && i < n)
+                        x[q] = csub(x[q], cmul(get(i, k), xk));
+                }
+            }
+            else
+            {
+                C part = cx<C>(0, 0);
+#pragma unroll
+                for(int q = 0; q < Q; ++q)
+                {
+                    const int j = lane + 32 * q;
+                    if((FWD ? q <= q0 : q >= q0) && (FWD ? j < k : j > k) && j < n)
+                    {
+                        const C t = cmul(get(k, j), x[q]);
+                        part = cx<C>(part.x + t.x, part.y + t.y);
+                    }
+                }
+#pragma unroll
+                for(int m = 16; m >= 1; m >>= 1)
+                {
+                    const C o = cshfl_xor(part, m);
+                    part = cx<C>(part.x + o.x, part.y + o.y);
+                }
+                if(lane == kk)
+                {
+                    const C v = csub(x[q0], part);
+                    x[q0] = UNIT ? v : cdiv(v, get(k, k));
+                }
+            }
+        }
+    }
+}
+
+// source position of each of this lane's rows under the interchanges piv[0..n-1] applied in
+// order (LAPACK laswp, incx = 1): position i holds original row src(i)
+template <int Q>
+__device__ __forceinline__ void warp_perm_src_q(const int* piv, int n, int (&src)[Q])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for(int q = 0; q < Q; ++q)
+        src[q] = lane + 32 * q;
+    for(int k = n - 1; k >= 0; --k)
+    {
+        const int p = piv[k] - 1;
+        RSB_CHECK_PIV(piv[k], n, __LINE__);
+#pragma unroll
+        for(int q = 0; q < Q; ++q)
+            src[q] = src[q] == k ? p : (src[q] == p ? k : src[q]);
+    }
+}
+
+// getrs with one warp per (member, right-hand-side column); four warps per CTA
+template <typename C, int Q>
+__global__ void __launch_bounds__(128)
+    cgetrs_warp_kernel(int trans, int n, int nrhs, Batch<C> A, int lda, const int* ipiv,
+                       int64_t strideP, Batch<C> B, int ldb, const int* skip, Gate gate,
+                       int64_t tasks)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t task = (int64_t)blockIdx.x * 4 + warp;
+    if(task >= tasks)
+        return;
+    const int64_t b = task / nrhs;
+    const int col = (int)(task % nrhs);
+    if((skip && skip[b] != 0) || gate.skip(b))
+        return;
+    const C* a = A.at(b);
+    C* xb = B.at(b);
+    int src[Q];
+    if(ipiv)
+        warp_perm_src_q<Q>(ipiv + b * strideP, n, src);
+    else
+#pragma unroll
+        for(int q = 0; q < Q; ++q)
+            src[q] = lane + 32 * q;
+    C x[Q];
+    const bool cj = trans == 2;
+#pragma unroll
+    for(int q = 0; q < Q; ++q)
+    {
+        const int i = lane + 32 * q;
+        x[q] = i < n ? RSB_AT(xb, trans == 0 ? src[q] : i, col, ldb, n, nrhs) : cx<C>(0, 0);
+    }
+    if(trans == 0)
+    {
+        // L y = P b (unit lower, columns of L), U x = y (columns of U)
+        auto el = [&](int i, int k) { return RSB_AT(a, i, k, lda, n, n); };
+        warp_trsv<C, Q, true, true, true>(n, x, el);
+        warp_trsv<C, Q, false, true, false>(n, x, el);
+    }
+    else
+    {
+        // op(U)^T y = b: row i of U^T is column i of U (DOT, lanes over k); op(L)^T x = y
+        auto opT = [&](int i, int k) {
+            const C v = RSB_AT(a, k, i, lda, n, n);
+            return cj ? cconj(v) : v;
+        };
+        warp_trsv<C, Q, true, false, false>(n, x, opT);
+        warp_trsv<C, Q, false, false, true>(n, x, opT);
+    }
+    __syncwarp();
+#pragma unroll
+    for(int q = 0; q < Q; ++q)
+    {
+        const int i = lane + 32 * q;
+        if(i < n)
+            RSB_AT(xb, trans == 0 ? i : src[q], col, ldb, n, nrhs) = x[q];
+    }
+}
+
+// potrs with one warp per (member, right-hand-side column): lower L L^H: L y = b (columns of
+// L), L^H x = y (rows of L^H = conjugated columns of L, DOT); upper U^H U: U^H y = b (DOT on
+// conjugated columns of U), U x = y (columns of U)
+template <typename C, int Q>
+__global__ void __launch_bounds__(128)
+    cpotrs_warp_kernel(int upper, int n, int nrhs, Batch<C> A, int lda, Batch<C> B, int ldb,
+                       const int* skip, int64_t tasks)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t task = (int64_t)blockIdx.x * 4 + warp;
+    if(task >= tasks)
+        return;
+    const int64_t b = task / nrhs;
+    const int col = (int)(task % nrhs);
+    if(skip && skip[b] != 0)
+        return;
+    const C* a = A.at(b);
+    C* xb = B.at(b);
+    C x[Q];
+#pragma unroll
+    for(int q = 0; q < Q; ++q)
+    {
+        const int i = lane + 32 * q;
+        x[q] = i < n ? RSB_AT(xb, i, col, ldb, n, nrhs) : cx<C>(0, 0);
+    }
+    auto el = [&](int i, int k) { return RSB_AT(a, i, k, lda, n, n); };
+    auto elH = [&](int i, int k) { return cconj(RSB_AT(a, k, i, lda, n, n)); };
+    if(upper)
+    {
+        warp_trsv<C, Q, true, false, false>(n, x, elH);
+        warp_trsv<C, Q, false, true, false>(n, x, el);
+    }
+    else
+    {
+        warp_trsv<C, Q, true, true, false>(n, x, el);
+        warp_trsv<C, Q, false, false, false>(n, x, elH);
+    }
+#pragma unroll
+    for(int q = 0; q < Q; ++q)
+    {
+        const int i = lane + 32 * q;
+        if(i < n)
+            RSB_AT(xb, i, col, ldb, n, nrhs) = x[q];
+    }
+}
+
 inline rocblas_status status_of_launch()
 {
     return cudaGetLastError() == cudaSuccess ? rocblas_status_success
@@ -380,6 +666,17 @@ template <typename C>
 rocblas_status cx_getrf(cudaStream_t s, int m, int n, Batch<C> A, int lda, int* ipiv,
                         int64_t sP, int* info, int bc, bool pivot, Gate g)
 {
+    const size_t bytes = sizeof(C) * (size_t)m * n;
+    if(bytes <= CPX_SMEM_MAX)
+    {
+        RSB_LOG_KERNEL("cgetrf_smem_kernel");
+        auto k = pivot ? cgetrf_smem_kernel<C, true> : cgetrf_smem_kernel<C, false>;
+        if(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, CPX_SMEM_MAX)
+           != cudaSuccess)
+            return rocblas_status_internal_error;
+        k<<<bc, CPX_NT, bytes, s>>>(m, n, A, lda, ipiv, sP, info, g);
+        return status_of_launch();
+    }
     RSB_LOG_KERNEL("cgetrf_kernel");
     if(pivot)
         cgetrf_kernel<C, true><<<bc, CPX_NT, 0, s>>>(m, n, A, lda, ipiv, sP, info, g);
@@ -392,6 +689,25 @@ rocblas_status cx_getrs(cudaStream_t s, int trans, int n, int nrhs, Batch<C> A, 
                         const int* ipiv, int64_t sP, Batch<C> B, int ldb, const int* skip,
                         int bc, Gate g)
 {
+    if(n <= 256)
+    {
+        RSB_LOG_KERNEL("cgetrs_warp_kernel");
+        const int64_t tasks = (int64_t)bc * nrhs;
+        const unsigned grid = (unsigned)((tasks + 3) / 4);
+        if(n <= 32)
+            cgetrs_warp_kernel<C, 1><<<grid, 128, 0, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B,
+                                                          ldb, skip, g, tasks);
+        else if(n <= 64)
+            cgetrs_warp_kernel<C, 2><<<grid, 128, 0, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B,
+                                                          ldb, skip, g, tasks);
+        else if(n <= 128)
+            cgetrs_warp_kernel<C, 4><<<grid, 128, 0, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B,
+                                                          ldb, skip, g, tasks);
+        else
+            cgetrs_warp_kernel<C, 8><<<grid, 128, 0, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B,
+                                                          ldb, skip, g, tasks);
+        return status_of_launch();
+    }
     RSB_LOG_KERNEL("cgetrs_kernel");
     cgetrs_kernel<C><<<bc, CPX_NT, 0, s>>>(trans, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, g);
     return status_of_launch();
@@ -399,6 +715,17 @@ rocblas_status cx_getrs(cudaStream_t s, int trans, int n, int nrhs, Batch<C> A, 
 template <typename C>
 rocblas_status cx_potrf(cudaStream_t s, int upper, int n, Batch<C> A, int lda, int* info, int bc)
 {
+    const size_t bytes = sizeof(C) * (size_t)n * n;
+    if(bytes <= CPX_SMEM_MAX)
+    {
+        RSB_LOG_KERNEL("cpotrf_smem_kernel");
+        if(cudaFuncSetAttribute(cpotrf_smem_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                CPX_SMEM_MAX)
+           != cudaSuccess)
+            return rocblas_status_internal_error;
+        cpotrf_smem_kernel<C><<<bc, CPX_NT, bytes, s>>>(upper, n, A, lda, info);
+        return status_of_launch();
+    }
     RSB_LOG_KERNEL("cpotrf_kernel");
     cpotrf_kernel<C><<<bc, CPX_NT, 0, s>>>(upper, n, A, lda, info);
     return status_of_launch();
@@ -407,6 +734,25 @@ template <typename C>
 rocblas_status cx_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<C> A, int lda,
                         Batch<C> B, int ldb, const int* skip, int bc)
 {
+    if(n <= 256)
+    {
+        RSB_LOG_KERNEL("cpotrs_warp_kernel");
+        const int64_t tasks = (int64_t)bc * nrhs;
+        const unsigned grid = (unsigned)((tasks + 3) / 4);
+        if(n <= 32)
+            cpotrs_warp_kernel<C, 1><<<grid, 128, 0, s>>>(upper, n, nrhs, A, lda, B, ldb, skip,
+                                                          tasks);
+        else if(n <= 64)
+            cpotrs_warp_kernel<C, 2><<<grid, 128, 0, s>>>(upper, n, nrhs, A, lda, B, ldb, skip,
+                                                          tasks);
+        else if(n <= 128)
+            cpotrs_warp_kernel<C, 4><<<grid, 128, 0, s>>>(upper, n, nrhs, A, lda, B, ldb, skip,
+                                                          tasks);
+        else
+            cpotrs_warp_kernel<C, 8><<<grid, 128, 0, s>>>(upper, n, nrhs, A, lda, B, ldb, skip,
+                                                          tasks);
+        return status_of_launch();
+    }
     RSB_LOG_KERNEL("cpotrs_kernel");
     cpotrs_kernel<C><<<bc, CPX_NT, 0, s>>>(upper, n, nrhs, A, lda, B, ldb, skip);
     return status_of_launch();

@@ -88,7 +88,7 @@ rocblas_status launch_getri(cudaStream_t s, int n, Batch<T> A, int lda, const in
     }
     if(cudaGetLastError() != cudaSuccess)
         return rocblas_status_internal_error;
-    rocblas_status st = launch_getrs<T>(s, 0, n, n, A, lda, ipiv, strideP, W, ldw, info, bc);
+    rocblas_status st = launch_getrs_many<T>(s, n, n, A, lda, ipiv, strideP, W, ldw, info, bc);
     if(st != rocblas_status_success || !inplace)
         return st;
     RSB_LOG_KERNEL("getri_copy_back_kernel");

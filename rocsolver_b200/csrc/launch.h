@@ -1,5 +1,5 @@
 // launch.h -- host-side launchers of the factor/solve kernels (internal interface between
-// the C-ABI layer in api.cpp and the CUDA translation units).
+// the C-ABI layer in api.cu and the CUDA translation units).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -31,6 +31,11 @@ template <typename T>
 rocblas_status launch_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T> A, int lda,
                             Batch<T> B, int ldb, const int* skip_info, int bc);
 rocblas_status launch_reset_info(cudaStream_t s, int* info, int bc);
+// getrs (trans N) tuned for many right-hand sides (getri)
+template <typename T>
+rocblas_status launch_getrs_many(cudaStream_t s, int n, int nrhs, Batch<T> A, int lda,
+                                 const int* ipiv, int64_t strideP, Batch<T> B, int ldb,
+                                 const int* skip_info, int bc);
 
 // the complex precisions (complex.cu); getrs takes trans 2 = conjugate transpose
 #define RSB_DECLARE_COMPLEX_LAUNCHERS(C)                                                      \

@@ -473,6 +473,19 @@ rocblas_status launch_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T>
                      : run_potrs<T, 4>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
 }
 
+// Solve with many right-hand sides (getri's n columns of the identity): 32 columns per CTA
+// through shared memory for 32 < n <= 512, so that each CTA's pass over the factors (and its
+// diagonal-block inversions) serves 32 columns instead of 4; otherwise launch_getrs.
+template <typename T>
+rocblas_status launch_getrs_many(cudaStream_t s, int n, int nrhs, Batch<T> A, int lda,
+                                 const int* ipiv, int64_t sP, Batch<T> B, int ldb,
+                                 const int* skip, int bc)
+{
+    if(n <= 32 || n > 512 || nrhs < 32)
+        return launch_getrs<T>(s, 0, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, no_gate());
+    return run_getrs_cta<T, 32>(s, 0, n, nrhs, A, lda, ipiv, sP, B, ldb, skip, bc, no_gate());
+}
+
 // ------------------------------------------------------------------------------ instances
 #define RSB_INST(T)                                                                          \
     template rocblas_status launch_getrf<T>(cudaStream_t, int, int, Batch<T>, int, int*,   \
@@ -485,7 +498,10 @@ rocblas_status launch_potrs(cudaStream_t s, int upper, int n, int nrhs, Batch<T>
     template rocblas_status launch_potrf<T>(cudaStream_t, int, int, Batch<T>, int, int*,   \
                                             int);                                          \
     template rocblas_status launch_potrs<T>(cudaStream_t, int, int, int, Batch<T>, int,    \
-                                            Batch<T>, int, const int*, int);
+                                            Batch<T>, int, const int*, int);               \
+    template rocblas_status launch_getrs_many<T>(cudaStream_t, int, int, Batch<T>, int,    \
+                                                 const int*, int64_t, Batch<T>, int,       \
+                                                 const int*, int);
 RSB_INST(float)
 RSB_INST(double)
 

@@ -358,3 +358,54 @@ def test_empty_and_quick_returns(handle, P):
     np.testing.assert_array_equal(host(dI), [0, 0])
     _call(f"rocsolver_{P}getrs_strided_batched", handle, rs.OP_C, 0, 1, None, 1, 0, None, 1,
           None, 1, 0, 2)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+@pytest.mark.parametrize("n", [70, 257, 300])
+def test_kernel_boundaries(handle, P, n):
+    """Sizes on both sides of the shared-memory factorisation limit (96 KB per member) and of
+    the warp solves (n <= 256): getrf, getrs with N / T / C and potrf / potrs (lower and
+    upper) against the oracle."""
+    bc, nrhs = 2, 3
+    A = uniform_complex(n, n, bc, seed=900 + n).astype(DT[P])
+    B = uniform_complex(n, nrhs, bc, seed=901 + n).astype(DT[P])
+    LU, ipiv, info = gpu_getrf(handle, P, A)
+    oLU, oipiv, oinfo = oracle_getrf(A)
+    np.testing.assert_array_equal(info, oinfo)
+    if P == "z":
+        np.testing.assert_array_equal(ipiv, oipiv)
+    for b in range(bc):
+        if np.array_equal(ipiv[b], oipiv[b]):
+            assert norm_error("F", oLU[b], LU[b]) <= 4 * n * eps(P)
+    fLU, fP = to_colmajor(LU), ipiv.reshape(-1).astype(np.int32).copy()
+    for trans in (0, 1, 2):
+        oB = to_colmajor(B)
+        oracle.cgetrs(trans, n, nrhs, fLU.copy(), n, n * n, fP.copy(), n, oB, n, n * nrhs, bc)
+        dA, dB, dP = dev(fLU), dev(to_colmajor(B)), dev(fP)
+        _call(f"rocsolver_{P}getrs_strided_batched", handle, OPS[trans], n, nrhs, ptr(dA), n,
+              n * n, ptr(dP), n, ptr(dB), n, n * nrhs, bc)
+        X = from_colmajor(host(dB), bc, n, nrhs, n, n * nrhs)
+        oX = from_colmajor(oB, bc, n, nrhs, n, n * nrhs)
+        for b in range(bc):
+            assert norm_error("I", oX[b], X[b]) <= 20 * n * eps(P), (trans, b)
+    H = hpd_gram(n, bc, seed=902 + n).astype(DT[P])
+    for lower in (True, False):
+        C, info, dC = gpu_potrf(handle, P, H, lower)
+        oC = to_colmajor(H)
+        oI = np.zeros(bc, np.int32)
+        oracle.cpotrf(not lower, n, oC, n, n * n, oI, bc)
+        np.testing.assert_array_equal(info, oI)
+        f = norm_error_lower if lower else norm_error_upper
+        oCm = from_colmajor(oC, bc, n, n, n, n * n)
+        for b in range(bc):
+            assert f("F", oCm[b], C[b]) <= n * eps(P)
+        dB = dev(to_colmajor(B))
+        uplo = rs.FILL_LOWER if lower else rs.FILL_UPPER
+        _call(f"rocsolver_{P}potrs_strided_batched", handle, uplo, n, nrhs, ptr(dC), n, n * n,
+              ptr(dB), n, n * nrhs, bc)
+        oB = to_colmajor(B)
+        oracle.cpotrs(not lower, n, nrhs, oC, n, n * n, oB, n, n * nrhs, bc)
+        X = from_colmajor(host(dB), bc, n, nrhs, n, n * nrhs)
+        oX = from_colmajor(oB, bc, n, nrhs, n, n * nrhs)
+        for b in range(bc):
+            assert norm_error("I", oX[b], X[b]) <= 20 * n * eps(P), (lower, b)
