@@ -27,6 +27,10 @@ configurations; no dataset is involved):
   adjoint_n128   n=128, batch 8192, nrhs 8, FP64, A ~ U[-1,1] + 4 I factored once outside
               the timing, G ~ N(0,1): rocsolver_dgetrs_adjoint_strided_batched (gB, gA).
   adjoint_n128_fp32  the same in FP32 (rocsolver_sgetrs_adjoint_strided_batched).
+  zgesv_n64   complex double, n=64, batch 8192, nrhs 1, real and imaginary parts of A and b
+              ~ U[-1,1]: rocsolver_zgesv_strided_batched.
+  getri_n64   n=64, batch 16384, A ~ U[-1,1] + 4 I factored once outside the timing:
+              rocsolver_dgetri_strided_batched (inverse in place).
 Inputs are larger than L2 (126 MB) for gesv_n256 and potrf_n64; getrf_n32 (8 MB) rotates
 through 24 distinct copies of the batch so each step reads cold data.
 
@@ -49,10 +53,13 @@ sys.path.insert(0, ROOT)
 
 
 WORKLOADS = ("dsgesv_n256", "gesv_n256", "getrf_n32", "potrf_n64", "vbatched_4096",
-             "adjoint_n128", "adjoint_n128_fp32")
+             "adjoint_n128", "adjoint_n128_fp32", "zgesv_n64", "getri_n64")
 EXTRA_WORKLOADS = ("vbatched_4096", "adjoint_n128", "adjoint_n128_fp32")
-# the workloads measured beside the headline in the default run (C1, C2, C4, C5)
-NESTED = ("getrf_n32", "potrf_n64", "vbatched_4096", "adjoint_n128", "adjoint_n128_fp32")
+WIDE_WORKLOADS = ("zgesv_n64", "getri_n64")  # the complex and inverse entry points
+# the workloads measured beside the headline in the default run (C1, C2, C4, C5, and the
+# complex solve and the inverse)
+NESTED = ("getrf_n32", "potrf_n64", "vbatched_4096", "adjoint_n128", "adjoint_n128_fp32",
+          "zgesv_n64", "getri_n64")
 
 
 def parse():
@@ -551,6 +558,8 @@ def _host_inputs(w):
         elif w.name.startswith("adjoint"):
             w.host = (w.A0.double().cpu().numpy(), w.X0.double().cpu().numpy(),
                       w.G0.double().cpu().numpy())
+        elif w.name == "getri_n64":
+            w.host = (w.A0.cpu().numpy(),)
         else:
             w.host = (w.A0.cpu().numpy(), w.B0.cpu().numpy())
     return w.host
@@ -588,6 +597,34 @@ def _lapack_run(w, routine, cnt, threads):
         oracle.lapack_batch(oracle.LH_ADJOINT, n, k, LU, n, n * n, piv, n, gB, n, n * k,
                             bc=cnt, nthreads=threads)
         oracle.lapack_outer(n, k, gB, X0[:cnt].reshape(-1), gA, cnt, nthreads=threads)
+        return time.perf_counter() - t0
+    if w.name == "zgesv_n64":
+        A0, B0 = _host_inputs(w)
+        n, k = w.n, w.nrhs
+        A = A0[:cnt].reshape(-1).view(np.float64).copy()
+        B = B0[:cnt].reshape(-1).view(np.float64).copy()
+        ipiv = np.zeros(cnt * n, np.int32)
+        info = np.zeros(cnt, np.int32)
+        t0 = time.perf_counter()
+        oracle.lapack_batch(oracle.LH_ZGESV, n, k, A, n, 2 * n * n, ipiv, n, B, n, 2 * n * k,
+                            info=info, bc=cnt, nthreads=threads)
+        return time.perf_counter() - t0
+    if w.name == "getri_n64":
+        (A0,) = _host_inputs(w)
+        n = w.n
+        if not hasattr(w, "host_lu"):  # factored once, outside the timing, like the GPU arm
+            LU = A0.reshape(-1).copy()
+            piv = np.zeros(w.bc * n, np.int32)
+            inf = np.zeros(w.bc, np.int32)
+            oracle.lapack_batch(oracle.LH_GETRF_GETRS, n, 0, LU, n, n * n, piv, n, None, n, 0,
+                                info=inf, bc=w.bc, nthreads=oracle.physical_cores())
+            w.host_lu = (LU, piv)
+        LU, piv = w.host_lu
+        A = LU[:cnt * n * n].copy()
+        info = np.zeros(cnt, np.int32)
+        t0 = time.perf_counter()
+        oracle.lapack_batch(oracle.LH_GETRI, n, 0, A, n, n * n, piv, n, None, n, 0, info=info,
+                            bc=cnt, nthreads=threads)
         return time.perf_counter() - t0
     A0, B0 = _host_inputs(w)
     n, k = w.n, w.nrhs
@@ -627,7 +664,8 @@ def _lapack_routines(w):
             "getrf_n32": ["getrf+getrs"], "potrf_n64": ["potrf+potrs"],
             "vbatched_4096": ["gesv (per-member n, nrhs)"],
             "adjoint_n128": ["getrs (trans T) + dgemm"],
-            "adjoint_n128_fp32": ["getrs (trans T) + dgemm"]}[w.name]
+            "adjoint_n128_fp32": ["getrs (trans T) + dgemm"],
+            "zgesv_n64": ["zgesv"], "getri_n64": ["getri (factors given)"]}[w.name]
 
 
 def cpu_sample(w, target_s, one_core_s=None):
@@ -730,6 +768,8 @@ def main():
 
 
 def run_workload(name, args, ctx, steps, warmup, cpu_seconds):
+    if name in WIDE_WORKLOADS:
+        return run_wide(name, args, ctx, steps, warmup, cpu_seconds)
     if name in EXTRA_WORKLOADS:
         return run_extra(name, args, ctx, steps, warmup, cpu_seconds)
     return run_core(name, args, ctx, steps, warmup, cpu_seconds)
@@ -851,6 +891,210 @@ def main_reference(args, rank, world):
 
 
 # ----------------------------------------------------------------------------- extra rows
+def run_wide(name, args, ctx, steps, warmup, cpu_seconds):
+    """The complex solve (zgesv_n64) and the inverse (getri_n64): same contract as run_core
+    (device time of the API call per step, max over ranks; e2e through the C ABI with host
+    buffers; roofline of the dominant kernel; host LAPACK beside it)."""
+    torch, rs, dev, pg, handle = ctx.torch, ctx.rs, ctx.dev, ctx.pg, ctx.handle
+    world, rank = ctx.world, ctx.rank
+    h = handle.value
+    P = rs.ptr
+    stream = torch.cuda.current_stream()
+    w = Workload()
+    w.name = name
+    g = torch.Generator(device=dev)
+    if name == "zgesv_n64":
+        n, bc, nrhs = 64, 8192, 1
+        g.manual_seed(13)
+        re = lambda *sh: torch.rand(*sh, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+        A = torch.complex(re(bc, n, n), re(bc, n, n))
+        B = torch.complex(re(bc, n, nrhs), re(bc, n, nrhs))
+        w.A0, w.B0 = colmajor(torch, A), colmajor(torch, B)
+        es = 16
+        w.metric = "batched complex solves/s (zgesv_strided_batched, n=64)"
+        w.unit = "solves/s"
+        w.dtype = "c128"
+        w.config = {"workload": "rocsolver_zgesv_strided_batched, n=64, batch 8192, nrhs 1, "
+                                "re/im of A and b ~ U[-1,1]", "n": n, "batch": bc, "nrhs": nrhs,
+                    "l2": "inputs 537 MB > L2; A and B restored between steps outside the "
+                          "timed events"}
+        w.bytes_per_unit = 2 * n * n * es + 4 * n + 4        # zgetrf: A in and out, ipiv, info
+        w.flops_per_unit = 8.0 * n ** 3 / 3 + 8.0 * n * n * nrhs
+        w.kernel = "cgetrf_smem_kernel<rocblas_double_complex> (member in shared memory)"
+        A_, B_ = w.A0.clone(), w.B0.clone()
+        ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
+        info = torch.zeros(bc, dtype=torch.int32, device=dev)
+
+        def call():
+            rs.check(rs.call("rocsolver_zgesv_strided_batched", h, n, nrhs, P(A_), n, n * n,
+                             P(ipiv), n, P(B_), n, n * nrhs, P(info), bc), "zgesv")
+
+        def kernel_only():
+            rs.check(rs.call("rocsolver_zgetrf_strided_batched", h, n, n, P(A_), n, n * n,
+                             P(ipiv), n, P(info), bc), "zgetrf")
+
+        def restore():
+            A_.copy_(w.A0)
+            B_.copy_(w.B0)
+        launches = 2
+    else:
+        n, bc, nrhs = 64, 16384, 0
+        g.manual_seed(14)
+        A = torch.rand(bc, n, n, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+        A += 4 * torch.eye(n, device=dev, dtype=torch.float64)
+        w.A0 = colmajor(torch, A)
+        es = 8
+        w.metric = "batched inverses/s (dgetri_strided_batched from the LU factors, n=64)"
+        w.unit = "inverses/s"
+        w.dtype = "f64"
+        w.config = {"workload": "rocsolver_dgetri_strided_batched in place, n=64, batch 16384, "
+                                "A ~ U[-1,1] + 4 I factored by dgetrf once outside the timing",
+                    "n": n, "batch": bc,
+                    "l2": "factors 537 MB > L2; restored between steps outside the timed events"}
+        w.bytes_per_unit = 2 * n * n * es + 4 * n + 4        # LU in, inverse out, ipiv, info
+        w.flops_per_unit = 4.0 * n ** 3 / 3
+        w.kernel = ("dgetri: getri_prep_kernel + getrs_cta_kernel<double, 64, 32> (A C = I, 32 "
+                    "columns of I per CTA) + getri_copy_back_kernel (kernel_ms = the whole call)")
+        LU0 = w.A0.clone()
+        ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
+        info = torch.zeros(bc, dtype=torch.int32, device=dev)
+        rs.check(rs.call("rocsolver_dgetrf_strided_batched", h, n, n, P(LU0), n, n * n, P(ipiv),
+                         n, P(info), bc), "dgetrf")
+        A_ = LU0.clone()
+
+        def call():
+            rs.check(rs.call("rocsolver_dgetri_strided_batched", h, n, P(A_), n, n * n, P(ipiv),
+                             n, P(info), bc), "dgetri")
+        kernel_only = call
+
+        def restore():
+            A_.copy_(LU0)
+        launches = 3
+    w.n, w.bc, w.nrhs = n, bc, nrhs
+    for _ in range(warmup):
+        restore()
+        call()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    time.sleep(0.3)
+    for i in range(steps):
+        restore()
+        ev[i][0].record(stream)
+        call()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(torch, pg, sum(a.elapsed_time(b) for a, b in ev), dev)
+    ms = total_ms / steps
+    kev = []
+    for _ in range(min(steps, 10)):
+        restore()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        kernel_only()
+        b.record(stream)
+        kev.append((a, b))
+    torch.cuda.synchronize()
+    kms = statistics.median([a.elapsed_time(b) for a, b in kev])
+    # accuracy of one more call
+    restore()
+    call()
+    torch.cuda.synchronize()
+    if name == "zgesv_n64":
+        Ar = w.A0.view(bc, n, n).transpose(1, 2)
+        X = B_.view(bc, nrhs, n).transpose(1, 2)
+        Bm = w.B0.view(bc, nrhs, n).transpose(1, 2)
+        R = torch.bmm(Ar, X) - Bm
+        num = R.abs().sum(2).amax(1)
+        den = Ar.abs().sum(2).amax(1) * X.abs().sum(2).amax(1) + Bm.abs().sum(2).amax(1)
+        berr = num / den
+        acc = {"backward_err_max": float(berr.max()),
+               "frac_backward_err_le_1e-13": float((berr <= 1e-13).double().mean()),
+               "info_nonzero": int((info != 0).sum())}
+    else:
+        Ar = w.A0.view(bc, n, n).transpose(1, 2)
+        Inv = A_.view(bc, n, n).transpose(1, 2)
+        E = torch.bmm(Ar, Inv) - torch.eye(n, device=dev, dtype=torch.float64)
+        rel = E.abs().amax((1, 2)) / (Ar.abs().sum(2).amax(1) * Inv.abs().sum(2).amax(1))
+        acc = {"residual_AinvA_minus_I_rel_max": float(rel.max()),
+               "info_nonzero": int((info != 0).sum())}
+    # e2e: inputs from pinned host memory, results back, every step (sliced over 2 streams)
+    if name == "zgesv_n64":
+        hA, hB = w.A0.cpu().pin_memory(), w.B0.cpu().pin_memory()
+        hX, hI = torch.empty_like(hB).pin_memory(), torch.empty(bc, dtype=torch.int32).pin_memory()
+        dA, dB = torch.empty_like(w.A0), torch.empty_like(w.B0)
+        h2d, d2h = (hA.numel() + hB.numel()) * es, hX.numel() * es + bc * 4
+
+        def body(hs, c0, c1):
+            sl_ = slice(c0, c1)
+            dA[sl_].copy_(hA[sl_], non_blocking=True)
+            dB[sl_].copy_(hB[sl_], non_blocking=True)
+            rs.check(rs.call("rocsolver_zgesv_strided_batched", hs, n, nrhs, P(dA[sl_]), n,
+                             n * n, P(ipiv.view(bc, n)[sl_]), n, P(dB[sl_]), n, n * nrhs,
+                             P(info[sl_]), c1 - c0), "zgesv")
+            hX[sl_].copy_(dB[sl_], non_blocking=True)
+            hI[sl_].copy_(info[sl_], non_blocking=True)
+    else:
+        hLU, hP = LU0.cpu().pin_memory(), ipiv.cpu().pin_memory()
+        hInv, hI = torch.empty_like(hLU).pin_memory(), torch.empty(bc, dtype=torch.int32).pin_memory()
+        dA, dP = torch.empty_like(LU0), torch.empty_like(ipiv)
+        h2d, d2h = hLU.numel() * es + hP.numel() * 4, hInv.numel() * es + bc * 4
+
+        def body(hs, c0, c1):
+            sl_ = slice(c0, c1)
+            dA[sl_].copy_(hLU[sl_], non_blocking=True)
+            dP.view(bc, n)[sl_].copy_(hP.view(bc, n)[sl_], non_blocking=True)
+            rs.check(rs.call("rocsolver_dgetri_strided_batched", hs, n, P(dA[sl_]), n, n * n,
+                             P(dP.view(bc, n)[sl_]), n, P(info[sl_]), c1 - c0), "dgetri")
+            hInv[sl_].copy_(dA[sl_], non_blocking=True)
+            hI[sl_].copy_(info[sl_], non_blocking=True)
+    sl = SlicedStep(torch, rs, bc, h2d + d2h, body)
+    try:
+        for _ in range(2):
+            sl.step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k = max(3, min(steps, 5))
+        a.record(sl.main)
+        for _ in range(k):
+            sl.step()
+        b.record(sl.main)
+        torch.cuda.synchronize()
+    finally:
+        sl.close()
+    e2e_ms = max_over_ranks(torch, pg, a.elapsed_time(b) / k, dev)
+    peaks = ctx.peaks
+    gbs = w.bytes_per_unit * bc / (kms / 1e3) / 1e9
+    tf = w.flops_per_unit * bc / (kms / 1e3) / 1e12
+    line = {"metric": w.metric, "value": bc * world / (ms / 1e3), "unit": w.unit,
+            "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
+            "data": "synthetic (seeded, generated on device)", "config": w.config,
+            "gpu_launches": launches * steps,
+            "e2e": {"value": bc * world / (e2e_ms / 1e3), "unit": w.unit,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "pipeline": sl.desc},
+            "roofline": {"bound": "hbm",
+                         "limiter": "latency: per-column barriers of one CTA per member"
+                         if name == "zgesv_n64" else
+                         "latency: blocked triangular sweeps, one CTA per 32 columns",
+                         "kernel": w.kernel, "achieved": gbs, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"], "traffic": None,
+                         "peak_source": peaks["source"], "kernel_ms": kms,
+                         "compute": {"achieved_tflops": tf, "peak_tflops": peaks["fp64_tflops"],
+                                     "frac": tf / peaks["fp64_tflops"],
+                                     "peak": "FP64 dgemm measured in this run (cuBLAS 8192^3)"}},
+            "clocks": clocks, "accuracy": acc}
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_sample(w, cpu_seconds)
+    return line
+
+
 def _vb_inputs(torch, dev, bc, nmax, seed):
     g = torch.Generator(device=dev)
     g.manual_seed(seed)

@@ -147,7 +147,8 @@ def refgen(count):
 # Host LAPACK (OpenBLAS as bundled with scipy, loaded with dlopen by oracle/lapack_host.c):
 # the reference's own CPU path for these routines, timed as the CPU baseline.  One LAPACK
 # call per member on one thread, the batch split statically over nthreads pthreads.
-LH_GETRF_GETRS, LH_POTRF_POTRS, LH_GESV, LH_DSGESV, LH_ADJOINT, LH_GETRI, LH_VGESV = range(7)
+(LH_GETRF_GETRS, LH_POTRF_POTRS, LH_GESV, LH_DSGESV, LH_ADJOINT, LH_GETRI, LH_VGESV,
+ LH_ZGESV) = range(8)
 _lh_ready = False
 
 

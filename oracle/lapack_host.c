@@ -19,6 +19,8 @@
  *   LH_ADJOINT     : dgetrs ('T') on G in the B slot (gB = A^-T G, A holding LU factors
  *                    and ipiv); the outer product gA = -gB X^T is lapack_host_outer (dgemm)
  *   LH_GETRI       : dgetri per member (A holding LU factors and ipiv)
+ *   LH_ZGESV       : zgesv per member (complex double, interleaved re/im: A, B, the strides
+ *                    sA / sB counted in doubles, lda / ldb in complex elements)
  *   LH_VGESV       : dgesv per member with per-member order n[b] and nrhs[b] (members in
  *                    fixed slots of strideA / strideB elements, lda = ldb = ld)
  */
@@ -36,7 +38,8 @@ enum
     LH_DSGESV = 3,
     LH_ADJOINT = 4,
     LH_GETRI = 5,
-    LH_VGESV = 6
+    LH_VGESV = 6,
+    LH_ZGESV = 7
 };
 
 typedef void (*getrf_t)(const int*, const int*, double*, const int*, int*, int*);
@@ -67,6 +70,7 @@ static struct
     getri_t getri;
     gemm_t gemm;
     setnt_t setnt;
+    gesv_t zgesv; /* same argument list with complex (interleaved) arrays */
 } L;
 
 /* Load the LAPACK library at path (once).  Returns 0 on success, else the number of the
@@ -80,9 +84,9 @@ int lapack_host_open(const char* path)
         return -1;
     const char* names[] = {"scipy_dgetrf_", "scipy_dgetrs_", "scipy_dpotrf_", "scipy_dpotrs_",
                            "scipy_dgesv_",  "scipy_dsgesv_", "scipy_dgetri_", "scipy_dgemm_",
-                           "scipy_openblas_set_num_threads"};
-    void* f[9];
-    for(int i = 0; i < 9; ++i)
+                           "scipy_openblas_set_num_threads", "scipy_zgesv_"};
+    void* f[10];
+    for(int i = 0; i < 10; ++i)
     {
         f[i] = dlsym(h, names[i]);
         if(!f[i])
@@ -100,6 +104,7 @@ int lapack_host_open(const char* path)
     L.getri = (getri_t)f[6];
     L.gemm = (gemm_t)f[7];
     L.setnt = (setnt_t)f[8];
+    L.zgesv = (gesv_t)f[9];
     L.setnt(1);
     L.h = h;
     return 0;
@@ -166,6 +171,7 @@ static void* run_slice(void* arg)
             }
             break;
         case LH_GESV: L.gesv(&n, &nrhs, a, &j->lda, p, bb, &j->ldb, &inf); break;
+        case LH_ZGESV: L.zgesv(&n, &nrhs, a, &j->lda, p, bb, &j->ldb, &inf); break;
         case LH_DSGESV:
             L.dsgesv(&n, &nrhs, a, &j->lda, p, bb, &j->ldb, x, &j->ldx, work, swork, &it, &inf);
             if(j->iter)

@@ -78,35 +78,41 @@ __device__ __forceinline__ C cdiv(C a, C b)
     return cx<C>((a.x * r + a.y) / d, (a.y * r - a.x) / d);
 }
 
-// CTA-wide (key, row) argmax: largest key, smallest row on ties (LAPACK izamax order)
-template <typename K>
-__device__ int cta_argmax(K key, int row, bool valid, K* skey, int* srow)
+// 1 / z for |z| >= sfmin with one real division: z scaled by the power of two 2^-e of its
+// larger component (exact), 1/z = conj(z') / |z'|^2 * 2^-e
+template <typename C>
+__device__ __forceinline__ C crcp(C z)
 {
-    K wk;
-    const int wr = warp_argmax(key, row, valid, &wk);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if(lane == 0)
-    {
-        skey[warp] = wk;
-        srow[warp] = wr;
-    }
-    __syncthreads();
-    const bool rv = lane < CPX_NT / 32 && srow[lane] != INT_MAX;
-    K gk;
-    const int gr = warp_argmax(rv ? skey[lane] : K(0), rv ? srow[lane] : INT_MAX, rv, &gk);
-    __syncthreads();
-    return gr;
+    using R = typename CxReal<C>::R;
+    const int e = ilogb(fmax(fabs(z.x), fabs(z.y)));
+    const R x = scalbn(z.x, -e), y = scalbn(z.y, -e);
+    const R inv = R(1) / (x * x + y * y);
+    return cx<C>(scalbn(x * inv, -e), scalbn(-y * inv, -e));
 }
 
+// pivot-search records of one column, double-buffered by column parity so that the next
+// column's records never overwrite ones still being read
+template <typename C>
+struct CxPivRec
+{
+    using K = typename KeyOf<typename CxReal<C>::R>::type;
+    K key[2][CPX_NT / 32];
+    int row[2][CPX_NT / 32];
+    C val[2][CPX_NT / 32];
+    C ajj[2];
+};
+
 // LU of one m x n member at a (leading dimension lda: global memory, or the member's copy in
-// shared memory) by the whole CTA; writes ipiv (PIVOT) and returns info.  Per column: the
-// pivot search over the rows (threads over rows, cta_argmax), the interchange over all
-// columns, the scaling of the column below the diagonal, and the rank-1 update of the
-// trailing matrix with warps over columns and lanes over rows (consecutive rows of a column
-// are contiguous: coalesced in global memory, conflict-free rows in shared memory).
+// shared memory) by the whole CTA; writes ipiv (PIVOT) and returns info.  Per column, three
+// barriers: (1) the pivot search over the rows (threads over rows; each warp's winner
+// publishes its key, row and value, thread 0 the diagonal entry), (2) the interchange of the
+// other columns, together with the scaling of the column below the diagonal (the pivot row's
+// slot takes the old diagonal entry), (3) the rank-1 update of the trailing matrix with warps
+// over columns and lanes over rows (consecutive rows of a column are contiguous: coalesced in
+// global memory, conflict-free rows in shared memory).
 template <typename C, bool PIVOT>
-__device__ int cgetrf_dev(int m, int n, C* a, int lda, int* piv,
-                          typename KeyOf<typename CxReal<C>::R>::type* skey, int* srow)
+__device__ __forceinline__ int cgetrf_dev(int m, int n, C* a, int lda, int* piv,
+                                          CxPivRec<C>& rec)
 {
     using R = typename CxReal<C>::R;
     using K = typename KeyOf<R>::type;
@@ -116,52 +122,81 @@ __device__ int cgetrf_dev(int m, int n, C* a, int lda, int* piv,
     int inf = 0;
     for(int j = 0; j < mn; ++j)
     {
-        int p = j;
-        if(PIVOT)
+        const int buf = j & 1;
+        // ---- (1) pivot search: this thread's first largest |re| + |im| among its rows
+        const int rend = PIVOT ? m : j + 1; // rows searched: j .. rend-1
+        if(j + warp * 32 >= rend)
         {
-            // this thread's first largest |re| + |im| among rows j + tid, j + tid + NT, ...
+            // no candidate row in this warp (for any of its strided passes when m > NT the
+            // first pass already has one)
+            if(lane == 0)
+                rec.row[buf][warp] = INT_MAX;
+        }
+        else
+        {
             K bk = 0;
             int br = INT_MAX;
-            for(int i = j + tid; i < m; i += CPX_NT)
+            C bv = cx<C>(0, 0);
+            for(int i = j + tid; i < rend; i += CPX_NT)
             {
                 const C v = RSB_AT(a, i, j, lda, m, n);
+                if(i == j)
+                    rec.ajj[buf] = v;
                 const K k = pivot_key((R)(fabs(v.x) + fabs(v.y)), i == j);
                 if(br == INT_MAX || k > bk)
                 {
                     bk = k;
                     br = i;
+                    bv = v;
                 }
             }
-            p = cta_argmax(bk, br, br != INT_MAX, skey, srow);
-            if(tid == 0)
-                piv[j] = p + 1;
+            K wk;
+            const int wr = warp_argmax(bk, br, br != INT_MAX, &wk);
+            if(br == wr && br != INT_MAX)
+            {
+                rec.key[buf][warp] = wk;
+                rec.row[buf][warp] = wr;
+                rec.val[buf][warp] = bv;
+            }
         }
-        const C pv = RSB_AT(a, p, j, lda, m, n);
         __syncthreads();
+        const bool rv = lane < NW && rec.row[buf][lane] != INT_MAX;
+        K gk;
+        const int p = warp_argmax(rv ? rec.key[buf][lane] : K(0),
+                                  rv ? rec.row[buf][lane] : INT_MAX, rv, &gk);
+        const int gw = __ffs(__ballot_sync(0xffffffffu, rv && rec.row[buf][lane] == p)) - 1;
+        const C pv = rec.val[buf][gw];
+        const C ajj = rec.ajj[buf];
+        if(PIVOT && tid == 0)
+            piv[j] = p + 1;
+        // ---- (2) interchange rows j and p outside column j; scale column j below the pivot
         if(!czero(pv))
         {
-            if(p != j)
-            {
+            if(p != j && tid < n)
                 for(int c = tid; c < n; c += CPX_NT)
-                {
-                    const C t = RSB_AT(a, j, c, lda, m, n);
-                    RSB_AT(a, j, c, lda, m, n) = RSB_AT(a, p, c, lda, m, n);
-                    RSB_AT(a, p, c, lda, m, n) = t;
-                }
-                __syncthreads();
-            }
-            const bool rec = hypot(pv.x, pv.y) >= Lim<R>::sfmin();
-            const C r = rec ? cdiv(cx<C>(1, 0), pv) : pv;
-            for(int i = j + 1 + tid; i < m; i += CPX_NT)
+                    if(c != j)
+                    {
+                        const C t = RSB_AT(a, j, c, lda, m, n);
+                        RSB_AT(a, j, c, lda, m, n) = RSB_AT(a, p, c, lda, m, n);
+                        RSB_AT(a, p, c, lda, m, n) = t;
+                    }
+            if(j + 1 + tid < m) // only threads with a row to scale form the reciprocal
             {
-                C& e = RSB_AT(a, i, j, lda, m, n);
-                e = rec ? cmul(e, r) : cdiv(e, pv);
+                const bool recip = hypot(pv.x, pv.y) >= Lim<R>::sfmin();
+                const C r = recip ? crcp(pv) : pv;
+                for(int i = j + 1 + tid; i < m; i += CPX_NT)
+                {
+                    C& e = RSB_AT(a, i, j, lda, m, n);
+                    e = recip ? cmul(i == p ? ajj : e, r) : cdiv(i == p ? ajj : e, pv);
+                }
             }
+            if(tid == 0)
+                RSB_AT(a, j, j, lda, m, n) = pv;
         }
         else if(inf == 0)
             inf = j + 1;
         __syncthreads();
-        // A(j+1:m, j+1:n) -= A(j+1:m, j) A(j, j+1:n)
+        // ---- (3) A(j+1:m, j+1:n) -= A(j+1:m, j) A(j, j+1:n)
         for(int c = j + 1 + warp; c < n; c += NW)
         {
             const C u = RSB_AT(a, j, c, lda, m, n);
@@ -183,14 +218,12 @@ __global__ void __launch_bounds__(CPX_NT)
     cgetrf_kernel(int m, int n, Batch<C> A, int lda, int* ipiv, int64_t strideP, int* info,
                   Gate gate)
 {
-    using K = typename KeyOf<typename CxReal<C>::R>::type;
-    __shared__ K skey[CPX_NT / 32];
-    __shared__ int srow[CPX_NT / 32];
+    __shared__ CxPivRec<C> rec;
     const int64_t b = blockIdx.x;
     if(gate.skip(b))
         return;
     const int inf = cgetrf_dev<C, PIVOT>(m, n, A.at(b), lda, PIVOT ? ipiv + b * strideP : nullptr,
-                                         skey, srow);
+                                         rec);
     if(threadIdx.x == 0)
         info[b] = inf;
 }
@@ -203,11 +236,9 @@ __global__ void __launch_bounds__(CPX_NT)
     cgetrf_smem_kernel(int m, int n, Batch<C> A, int lda, int* ipiv, int64_t strideP, int* info,
                        Gate gate)
 {
-    using K = typename KeyOf<typename CxReal<C>::R>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* sa = reinterpret_cast<C*>(smem_raw); // m x n, leading dimension m
-    __shared__ K skey[CPX_NT / 32];
-    __shared__ int srow[CPX_NT / 32];
+    __shared__ CxPivRec<C> rec;
     constexpr int NW = CPX_NT / 32;
     const int64_t b = blockIdx.x;
     if(gate.skip(b))
@@ -218,8 +249,7 @@ __global__ void __launch_bounds__(CPX_NT)
         for(int i = lane; i < m; i += 32)
             sa[i + (size_t)c * m] = RSB_AT(a, i, c, lda, m, n);
     __syncthreads();
-    const int inf = cgetrf_dev<C, PIVOT>(m, n, sa, m, PIVOT ? ipiv + b * strideP : nullptr, skey,
-                                         srow);
+    const int inf = cgetrf_dev<C, PIVOT>(m, n, sa, m, PIVOT ? ipiv + b * strideP : nullptr, rec);
     for(int c = warp; c < n; c += NW)
         for(int i = lane; i < m; i += 32)
             RSB_AT(a, i, c, lda, m, n) = sa[i + (size_t)c * m];
@@ -325,7 +355,7 @@ __global__ void __launch_bounds__(CPX_NT)
 // factorisation stops, as LAPACK zpotf2 does).  The other triangle is not touched.  The
 // trailing update runs with warps over columns and lanes over rows.
 template <typename C>
-__device__ int cpotrf_dev(int upper, int n, C* a, int lda)
+__device__ __forceinline__ int cpotrf_dev(int upper, int n, C* a, int lda)
 {
     using R = typename CxReal<C>::R;
     constexpr int NW = CPX_NT / 32;

@@ -5,7 +5,10 @@
 // U, then inv(A) L = inv(U) by blocked GEMM/TRSM, then column interchanges) and
 // roclapack_getri_outofplace.hpp:73-127 (check_singularity, C = I, getrs on C).
 //
-// B200 design: both forms solve A C = I with the library's getrs kernels (one warp per
+// B200 design: orders whose member fits in 64 KB of shared memory (FP64 n <= 90, FP32
+// n <= 128) are inverted on chip by one CTA per member with LAPACK's own unblocked steps
+// (getri_small_kernel: one pass over the factors in, one over the inverse out).  Larger
+// orders solve A C = I with the library's getrs kernels (one warp per
 // matrix and right-hand-side group for n <= 32, otherwise one CTA per matrix and group of
 // four columns, the factors staged through inverted diagonal blocks), after one prep kernel
 // that finds the first zero diagonal entry of U (info, LAPACK dtrtri's singularity test) and
@@ -70,15 +73,143 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// ---- small orders: the whole inverse in shared memory, one CTA (one thread per row) per
+// member, LAPACK's unblocked algorithm (dgetri = dtrti2 on U, then the solve of X L =
+// inv(U) column by column from the right, then the column interchanges in reverse order).
+// The member is read once and the inverse written once; no workspace.
+constexpr int GETRI_SMALL_BYTES = 64 * 1024;
+
+template <typename T>
+static bool getri_small(int n)
+{
+    return n <= 128 && (size_t)n * n * sizeof(T) <= GETRI_SMALL_BYTES;
+}
+
+// C.base == C.ptrs == nullptr: the inverse overwrites A.  Members whose U has a zero diagonal
+// entry get info = its order and keep A (getri_outofplace: C = I), as the prep kernel below.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT)
+    getri_small_kernel(int n, Batch<T> A, int lda, const int* ipiv, int64_t strideP,
+                       Batch<T> C, int ldc, int* info)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* s = reinterpret_cast<T*>(smem_raw); // n x n, leading dimension n
+    __shared__ int first;
+    const int64_t b = blockIdx.x;
+    const int i = threadIdx.x; // this thread's row
+    const T* a = A.at(b);
+    const bool inplace = C.base == nullptr && C.ptrs == nullptr;
+    T* out = inplace ? A.at(b) : C.at(b);
+    const int ldo = inplace ? lda : ldc;
+    if(i == 0)
+        first = INT_MAX;
+    __syncthreads();
+    if(i < n)
+    {
+        for(int c = 0; c < n; ++c)
+            s[i + c * n] = RSB_AT(a, i, c, lda, n, n);
+        if(s[i + i * n] == T(0))
+            atomicMin(&first, i);
+    }
+    __syncthreads();
+    if(first != INT_MAX)
+    {
+        if(!inplace && i < n)
+            for(int c = 0; c < n; ++c)
+                RSB_AT(out, i, c, ldo, n, n) = i == c ? T(1) : T(0);
+        if(i == 0)
+            info[b] = first + 1;
+        return;
+    }
+    // inv(U) in place (dtrti2, upper, non-unit): column j = -inv(U)(j,j) * inv(U_11) U(0:j, j)
+    for(int j = 0; j < n; ++j)
+    {
+        if(i == j)
+            s[j + j * n] = T(1) / s[j + j * n];
+        __syncthreads();
+        T t = T(0);
+        if(i < j)
+            for(int k = i; k < j; ++k)
+                t += s[i + k * n] * s[k + j * n];
+        const T ajj = -s[j + j * n];
+        __syncthreads();
+        if(i < j)
+            s[i + j * n] = t * ajj;
+    }
+    __syncthreads();
+    // X L = inv(U), columns from the right: X(:, j) -= X(:, j+1:n) L(j+1:n, j), L(:, j) -> 0
+    for(int j = n - 2; j >= 0; --j)
+    {
+        T t = T(0);
+        if(i < n)
+            for(int k = j + 1; k < n; ++k)
+                t += s[i + k * n] * s[k + j * n];
+        __syncthreads();
+        if(i < n)
+            s[i + j * n] = (i > j ? T(0) : s[i + j * n]) - t;
+        __syncthreads();
+    }
+    // column interchanges in reverse order, each thread on its own row
+    if(i < n)
+    {
+        if(ipiv)
+        {
+            const int* piv = ipiv + b * strideP;
+            for(int j = n - 2; j >= 0; --j)
+            {
+                const int jp = piv[j] - 1;
+                RSB_CHECK_PIV(piv[j], n, __LINE__);
+                if(jp != j && jp >= 0 && jp < n)
+                {
+                    const T tmp = s[i + j * n];
+                    s[i + j * n] = s[i + jp * n];
+                    s[i + jp * n] = tmp;
+                }
+            }
+        }
+        for(int c = 0; c < n; ++c)
+            RSB_AT(out, i, c, ldo, n, n) = s[i + c * n];
+    }
+    if(i == 0)
+        info[b] = 0;
+}
+
 size_t getri_workspace(int n, int bc, size_t elem, bool inplace)
 {
-    return inplace ? ws_round(elem * (size_t)n * n * bc) : 0;
+    const bool small = elem == sizeof(double) ? getri_small<double>(n) : getri_small<float>(n);
+    return inplace && !small ? ws_round(elem * (size_t)n * n * bc) : 0;
 }
 
 template <typename T>
 rocblas_status launch_getri(cudaStream_t s, int n, Batch<T> A, int lda, const int* ipiv,
                             int64_t strideP, Batch<T> C, int ldc, int* info, int bc, void* ws)
 {
+    if(getri_small<T>(n))
+    {
+        const size_t smem = sizeof(T) * (size_t)n * n;
+        RSB_LOG_KERNEL("getri_small_kernel");
+        if(n <= 64)
+        {
+            if(cudaFuncSetAttribute(getri_small_kernel<T, 64>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    GETRI_SMALL_BYTES)
+               != cudaSuccess)
+                return rocblas_status_internal_error;
+            getri_small_kernel<T, 64><<<bc, 64, smem, s>>>(n, A, lda, ipiv, strideP, C, ldc, info);
+        }
+        else
+        {
+            if(cudaFuncSetAttribute(getri_small_kernel<T, 128>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    GETRI_SMALL_BYTES)
+               != cudaSuccess)
+                return rocblas_status_internal_error;
+            getri_small_kernel<T, 128><<<bc, 128, smem, s>>>(n, A, lda, ipiv, strideP, C, ldc,
+                                                             info);
+        }
+        return cudaGetLastError() == cudaSuccess ? rocblas_status_success
+                                                 : rocblas_status_internal_error;
+    }
     const bool inplace = C.base == nullptr && C.ptrs == nullptr;
     Batch<T> W = inplace ? strided<T>(static_cast<T*>(ws), (int64_t)n * n) : C;
     const int ldw = inplace ? n : ldc;

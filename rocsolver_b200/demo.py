@@ -2,9 +2,11 @@
 
     python -m rocsolver_b200.demo --case getrf --n 256 --batch 512 [--dtype d] [--reps 3]
 
-Cases: getrf, getrs, gesv, potrf, potrs, dsgesv, adjoint, vbatched, sgetrf_tf32 (the FP32
-LU with split-TF32 trailing updates; its kernel configuration, the tcgen05 engine included,
-follows the tuning table, e.g. one named by $ROCSOLVER_B200_TUNING).  Used to drive
+Cases: getrf, getrs, gesv, potrf, potrs, getri (in place, from factors computed once before
+the timing), dsgesv, adjoint, vbatched, sgetrf_tf32 (the FP32 LU with split-TF32 trailing
+updates; its kernel configuration, the tcgen05 engine included, follows the tuning table,
+e.g. one named by $ROCSOLVER_B200_TUNING).  --dtype c / z runs the complex precisions of
+getrf, getrs, gesv, potrf and potrs.  Used to drive
 profilers (one small, fixed workload per kernel) and as a usage example of the C ABI from
 Python.  Prints the median device time per call.
 """
@@ -34,31 +36,39 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
                     choices=["getrf", "getrs", "gesv", "potrf", "potrs", "dsgesv", "adjoint",
-                             "vbatched", "sgetrf_tf32"])
+                             "vbatched", "sgetrf_tf32", "getri"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--nrhs", type=int, default=1)
-    ap.add_argument("--dtype", default="d", choices=["s", "d"])
+    ap.add_argument("--dtype", default="d", choices=["s", "d", "c", "z"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--cond", type=float, default=0.0,
                     help="dsgesv: A = U diag(s) V' with log10(cond) uniform in [1, COND]")
     a = ap.parse_args()
     if a.case == "sgetrf_tf32":
         a.dtype = "s"
-    dt = torch.float64 if a.dtype == "d" else torch.float32
+    dt = {"d": torch.float64, "s": torch.float32, "z": torch.complex128,
+          "c": torch.complex64}[a.dtype]
+    rdt = torch.float64 if a.dtype in "dz" else torch.float32
     dev = torch.device("cuda")
     g = torch.Generator(device=dev)
     g.manual_seed(0)
     n, bc, nrhs = a.n, a.batch, a.nrhs
-    A0 = torch.rand(bc, n, n, generator=g, device=dev, dtype=dt) * 2 - 1
+    def rnd(*shape):
+        x = torch.rand(*shape, generator=g, device=dev, dtype=rdt) * 2 - 1
+        if dt.is_complex:
+            x = torch.complex(x, torch.rand(*shape, generator=g, device=dev, dtype=rdt) * 2 - 1)
+        return x
+
+    A0 = rnd(bc, n, n)
     if a.case in ("potrf", "potrs"):
-        A0 = A0 @ A0.transpose(1, 2) + n * torch.eye(n, device=dev, dtype=dt)
+        A0 = A0 @ A0.conj().transpose(1, 2) + n * torch.eye(n, device=dev, dtype=dt)
     elif a.case == "dsgesv" and a.cond > 0:
         A0 = cond_matrices(torch, n, bc, g, dev, 1.0, a.cond)
-    elif a.case in ("dsgesv", "adjoint"):
+    elif a.case in ("dsgesv", "adjoint", "getri"):
         A0 = A0 + 4 * torch.eye(n, device=dev, dtype=dt)
     A0 = A0.transpose(1, 2).contiguous()
-    B0 = (torch.rand(bc, nrhs, n, generator=g, device=dev, dtype=dt) * 2 - 1).contiguous()
+    B0 = rnd(bc, nrhs, n).contiguous()
     A, B = A0.clone(), B0.clone()
     X = torch.empty_like(B)
     gA = torch.empty_like(A)
@@ -68,7 +78,7 @@ def main():
     p = a.dtype
     h = rs.Handle(torch.cuda.current_stream().cuda_stream)
     P = rs.ptr
-    if a.case in ("getrs", "adjoint"):
+    if a.case in ("getrs", "adjoint", "getri"):
         rs.check(rs.call(f"rocsolver_{p}getrf_strided_batched", h.value, n, n, P(A), n, n * n,
                          P(ipiv), n, P(info), bc), "getrf")
         A0 = A.clone()
@@ -107,6 +117,9 @@ def main():
         elif a.case == "potrs":
             st = rs.call(f"rocsolver_{p}potrs_strided_batched", h.value, rs.FILL_LOWER, n, nrhs,
                          P(A), n, n * n, P(B), n, n * nrhs, bc)
+        elif a.case == "getri":
+            st = rs.call(f"rocsolver_{p}getri_strided_batched", h.value, n, P(A), n, n * n,
+                         P(ipiv), n, P(info), bc)
         elif a.case == "dsgesv":
             st = rs.call("rocsolver_dsgesv_strided_batched", h.value, n, nrhs, P(A), n, n * n,
                          P(ipiv), n, P(B), n, n * nrhs, P(X), n, n * nrhs, P(it), P(info), bc)

@@ -193,13 +193,14 @@ def test_getri_bad_args(handle, p):
     assert rs.call(g, handle, 1, FAKE, 1, 1, NULL, 1, FAKE, 1, 1, FAKE, 1) == rs.INVALID_POINTER
     assert rs.call(f"rocsolver_{p}getri_npvt_outofplace_strided_batched", handle, 1, FAKE, 1, 1,
                    FAKE, 1, 1, NULL, 1) == rs.INVALID_POINTER
-    # in-place getri reports its workspace (n*n elements per member) to a size query
+    # in-place getri of an order too large for the on-chip inverse reports its workspace
+    # (n*n elements per member) to a size query
     sz = ctypes.c_size_t()
     assert rs.call("rocblas_start_device_memory_size_query", handle) == rs.SUCCESS
-    assert c(n=64, lda=64, sA=4096, sP=64, bc=10) == rs.SIZE_INCREASED
+    assert c(n=200, lda=200, sA=40000, sP=200, bc=10) == rs.SIZE_INCREASED
     assert rs.call("rocblas_stop_device_memory_size_query", handle, ctypes.byref(sz)) \
         == rs.SUCCESS
-    assert sz.value >= 64 * 64 * 10 * (8 if p == "d" else 4)
+    assert sz.value >= 200 * 200 * 10 * (8 if p == "d" else 4)
 
 
 @pytest.mark.parametrize("p", ["s", "d"])
