@@ -921,6 +921,10 @@ def run_wide(name, args, ctx, steps, warmup, cpu_seconds):
         w.bytes_per_unit = 2 * n * n * es + 4 * n + 4        # zgetrf: A in and out, ipiv, info
         w.flops_per_unit = 8.0 * n ** 3 / 3 + 8.0 * n * n * nrhs
         w.kernel = "cgetrf_smem_kernel<rocblas_double_complex> (member in shared memory)"
+        # 211.2 MB per 2048 members from `ncu --set full --clock-control none -k
+        # regex:cgetrf_smem -c 1 python -m rocsolver_b200.demo --case getrf --dtype z --n 64
+        # --batch 2048 --reps 2`
+        w.traffic_per_unit = (134246144 + 76958208) / 2048
         A_, B_ = w.A0.clone(), w.B0.clone()
         ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
         info = torch.zeros(bc, dtype=torch.int32, device=dev)
@@ -953,8 +957,11 @@ def run_wide(name, args, ctx, steps, warmup, cpu_seconds):
                     "l2": "factors 537 MB > L2; restored between steps outside the timed events"}
         w.bytes_per_unit = 2 * n * n * es + 4 * n + 4        # LU in, inverse out, ipiv, info
         w.flops_per_unit = 4.0 * n ** 3 / 3
-        w.kernel = ("dgetri: getri_prep_kernel + getrs_cta_kernel<double, 64, 32> (A C = I, 32 "
-                    "columns of I per CTA) + getri_copy_back_kernel (kernel_ms = the whole call)")
+        w.kernel = "getri_small_kernel<double, 64> (the whole inverse in shared memory)"
+        # 480.7 MB per 8192 members from `ncu --set full --clock-control none -k
+        # regex:getri_small -c 1 python -m rocsolver_b200.demo --case getri --n 64 --batch 8192
+        # --reps 2`
+        w.traffic_per_unit = (270556928 + 210124800) / 8192
         LU0 = w.A0.clone()
         ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
         info = torch.zeros(bc, dtype=torch.int32, device=dev)
@@ -969,7 +976,7 @@ def run_wide(name, args, ctx, steps, warmup, cpu_seconds):
 
         def restore():
             A_.copy_(LU0)
-        launches = 3
+        launches = 1
     w.n, w.bc, w.nrhs = n, bc, nrhs
     for _ in range(warmup):
         restore()
@@ -1080,11 +1087,12 @@ def run_wide(name, args, ctx, steps, warmup, cpu_seconds):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "pipeline": sl.desc},
             "roofline": {"bound": "hbm",
-                         "limiter": "latency: per-column barriers of one CTA per member"
+                         "limiter": "instructions and per-column barriers of one CTA per member"
                          if name == "zgesv_n64" else
-                         "latency: blocked triangular sweeps, one CTA per 32 columns",
+                         "latency: dependent dot-product chains in shared memory, 12 warps/SM",
                          "kernel": w.kernel, "achieved": gbs, "peak": peaks["hbm_gbs"],
-                         "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"], "traffic": None,
+                         "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
+                         "traffic": w.traffic_per_unit * bc,
                          "peak_source": peaks["source"], "kernel_ms": kms,
                          "compute": {"achieved_tflops": tf, "peak_tflops": peaks["fp64_tflops"],
                                      "frac": tf / peaks["fp64_tflops"],
