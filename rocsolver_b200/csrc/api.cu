@@ -84,7 +84,7 @@ rocblas_status getrs_impl(rocblas_handle h, rocblas_operation trans, int n, int 
         return rocblas_status_invalid_size;
     if(h->querying)
         return ws_query(h, 0);
-    if((n && !Aptr) || (n && !ipiv) || ((int64_t)nrhs * n && !Bptr))
+    if((n && !Aptr) || (n && !ipiv) || (nrhs && n && !Bptr))
         return rocblas_status_invalid_pointer;
     if(n == 0 || nrhs == 0 || bc == 0)
         return rocblas_status_success;
@@ -108,7 +108,7 @@ rocblas_status gesv_impl(rocblas_handle h, int n, int nrhs, Batch<T> A, const vo
         return rocblas_status_invalid_size;
     if(h->querying)
         return ws_query(h, 0);
-    if((n && !Aptr) || (n && !ipiv) || ((int64_t)nrhs * n && !Bptr) || (bc && !info))
+    if((n && !Aptr) || (n && !ipiv) || (nrhs && n && !Bptr) || (bc && !info))
         return rocblas_status_invalid_pointer;
     if(bc == 0)
         return rocblas_status_success;
@@ -156,7 +156,7 @@ rocblas_status potrs_impl(rocblas_handle h, rocblas_fill uplo, int n, int nrhs, 
         return rocblas_status_invalid_size;
     if(h->querying)
         return ws_query(h, 0);
-    if((n && !Aptr) || ((int64_t)nrhs * n && !Bptr))
+    if((n && !Aptr) || (nrhs && n && !Bptr))
         return rocblas_status_invalid_pointer;
     if(n == 0 || nrhs == 0 || bc == 0)
         return rocblas_status_success;
@@ -179,7 +179,7 @@ rocblas_status posv_impl(rocblas_handle h, rocblas_fill uplo, int n, int nrhs, B
         return rocblas_status_invalid_size;
     if(h->querying)
         return ws_query(h, 0);
-    if((n && !Aptr) || ((int64_t)nrhs * n && !Bptr) || (bc && !info))
+    if((n && !Aptr) || (nrhs && n && !Bptr) || (bc && !info))
         return rocblas_status_invalid_pointer;
     if(bc == 0)
         return rocblas_status_success;
@@ -235,7 +235,7 @@ rocblas_status gesv_outofplace_impl(rocblas_handle h, int n, int nrhs, T* A, int
         return rocblas_status_invalid_size;
     if(h->querying)
         return ws_query(h, 0);
-    if((n && !A) || (n && !ipiv) || ((int64_t)nrhs * n && !B) || ((int64_t)nrhs * n && !X)
+    if((n && !A) || (n && !ipiv) || (nrhs && n && !B) || (nrhs && n && !X)
        || !info)
         return rocblas_status_invalid_pointer;
     if(n == 0 || nrhs == 0)

@@ -829,7 +829,8 @@ __device__ __forceinline__ void getrf_cta_dev(int m, int n, T* a, int lda, int* 
             const int tm = UM ? 0 : (mt + 31) / 32, tn = ncp / 32;
             for(int t = warp; t < tm * tn; t += NW)
             {
-                const int r0 = (t % tm) * 32, cc0 = (t / tm) * 32;
+                const int tmd = tm > 0 ? tm : 1; // tm == 0 (UM) never enters the loop
+                const int r0 = (t % tmd) * 32, cc0 = (t / tmd) * 32;
                 Tile w;
                 int arow[4];
 #pragma unroll
@@ -902,7 +903,6 @@ __device__ __noinline__ void umma_update_k64(float* a, int lda, int r0, int kc0,
                                              UmCtx& um)
 {
     constexpr int KK = LU2_JO;
-    constexpr int TILE = 128 * KK;
     constexpr uint32_t SBO = (KK / 4) * 128;
     if(mt <= 0 || cfirst >= n || um.failed)
         return;
