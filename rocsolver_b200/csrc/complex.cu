@@ -228,6 +228,112 @@ __global__ void __launch_bounds__(CPX_NT)
         info[b] = inf;
 }
 
+// ---- m, n <= NMAX <= 32: one warp per member, lane i holds row i in registers (the real
+// getrf_warp_kernel's scheme).  Per column: every lane forms the reciprocal of its own
+// candidate while the warp reduction runs, the winner publishes its row (and reciprocal)
+// through a double-buffered shared-memory row ordered by __syncwarp, rows are relabelled
+// instead of moved, and each lane updates its own row.
+constexpr int CPX_WPB = 4; // members (warps) per CTA
+
+template <typename C, int NMAX, bool PIVOT>
+__global__ void __launch_bounds__(32 * CPX_WPB)
+    cgetrf_warp_kernel(int m, int n, Batch<C> A, int lda, int* ipiv, int64_t strideP,
+                       int* info, int bc, Gate gate)
+{
+    using R = typename CxReal<C>::R;
+    __shared__ C srow[CPX_WPB][2][NMAX + 1]; // pivot row; element NMAX: its reciprocal
+    __shared__ int sbig[CPX_WPB][2];         // |pivot| >= sfmin
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = (int64_t)blockIdx.x * CPX_WPB + warp;
+    if(b >= bc || gate.skip(b))
+        return;
+    C* a = A.at(b);
+    C r[NMAX];
+#pragma unroll
+    for(int j = 0; j < NMAX; ++j)
+        r[j] = (lane < m && j < n) ? RSB_AT(a, lane, j, lda, m, n) : cx<C>(0, 0);
+    int myrow = lane, mypiv = lane + 1, inf = 0;
+    const int mn = min(m, n);
+#pragma unroll
+    for(int k = 0; k < NMAX; ++k)
+    {
+        if(k < mn)
+        {
+        const int buf = k & 1;
+        C* row = srow[warp][buf];
+        // this lane's candidate: its reciprocal (used if it wins) formed off the serial path
+        const C x0 = r[k];
+        const bool big = hypot(x0.x, x0.y) >= Lim<R>::sfmin();
+        const C rc = big ? crcp(x0) : x0;
+        int prow = k;
+        if(PIVOT)
+            prow = warp_argmax_fast(pivot_key((R)(fabs(x0.x) + fabs(x0.y)), myrow == k), myrow,
+                                    lane < m && myrow >= k);
+        if(myrow == prow)
+        {
+#pragma unroll
+            for(int j = k; j < NMAX; ++j)
+                row[j] = r[j];
+            row[NMAX] = rc;
+            sbig[warp][buf] = big;
+        }
+        __syncwarp();
+        const C piv = row[k];
+        const C rcp = row[NMAX];
+        const bool pbig = sbig[warp][buf] != 0;
+        if(lane == k)
+            mypiv = prow + 1;
+        if(czero(piv) && inf == 0)
+            inf = k + 1;
+        if(PIVOT)
+        {
+            if(myrow == prow)
+                myrow = k;
+            else if(myrow == k)
+                myrow = prow;
+        }
+        if(lane < m && myrow > k)
+        {
+            // LAPACK zgetf2: multiply by the reciprocal when |pivot| >= sfmin, else divide;
+            // a zero pivot leaves the column unscaled
+            C l = r[k];
+            if(!czero(piv))
+                l = pbig ? cmul(l, rcp) : cdiv(l, piv);
+            r[k] = l;
+#pragma unroll
+            for(int j = k + 1; j < NMAX; ++j)
+                r[j] = csub(r[j], cmul(l, row[j]));
+        }
+        }
+    }
+    if(lane < m)
+    {
+#pragma unroll
+        for(int j = 0; j < NMAX; ++j)
+            if(j < n)
+                RSB_AT(a, myrow, j, lda, m, n) = r[j];
+    }
+    if(PIVOT && lane < mn)
+        ipiv[b * strideP + lane] = mypiv;
+    if(lane == 0)
+        info[b] = inf;
+}
+
+template <typename C, int NMAX>
+static rocblas_status cx_getrf_warp(cudaStream_t s, int m, int n, Batch<C> A, int lda,
+                                    int* ipiv, int64_t sP, int* info, int bc, bool pivot, Gate g)
+{
+    const unsigned grid = (unsigned)((bc + CPX_WPB - 1) / CPX_WPB);
+    if(pivot)
+        cgetrf_warp_kernel<C, NMAX, true><<<grid, 32 * CPX_WPB, 0, s>>>(m, n, A, lda, ipiv, sP,
+                                                                        info, bc, g);
+    else
+        cgetrf_warp_kernel<C, NMAX, false><<<grid, 32 * CPX_WPB, 0, s>>>(m, n, A, lda, ipiv, sP,
+                                                                         info, bc, g);
+    return cudaGetLastError() == cudaSuccess ? rocblas_status_success
+                                             : rocblas_status_internal_error;
+}
+
 // members of at most CPX_SMEM_MAX bytes are factored in shared memory (one copy in, one out)
 constexpr int CPX_SMEM_MAX = 96 * 1024;
 
@@ -696,6 +802,16 @@ template <typename C>
 rocblas_status cx_getrf(cudaStream_t s, int m, int n, Batch<C> A, int lda, int* ipiv,
                         int64_t sP, int* info, int bc, bool pivot, Gate g)
 {
+    if(m <= 32 && n <= 32)
+    {
+        RSB_LOG_KERNEL("cgetrf_warp_kernel");
+        const int mx = max(m, n);
+        if(mx <= 8)
+            return cx_getrf_warp<C, 8>(s, m, n, A, lda, ipiv, sP, info, bc, pivot, g);
+        if(mx <= 16)
+            return cx_getrf_warp<C, 16>(s, m, n, A, lda, ipiv, sP, info, bc, pivot, g);
+        return cx_getrf_warp<C, 32>(s, m, n, A, lda, ipiv, sP, info, bc, pivot, g);
+    }
     const size_t bytes = sizeof(C) * (size_t)m * n;
     if(bytes <= CPX_SMEM_MAX)
     {
