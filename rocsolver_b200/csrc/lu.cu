@@ -456,8 +456,6 @@ static rocblas_status run_potrs(cudaStream_t s, int upper, int n, int nrhs, Batc
         return run_potrs_small<T, 32, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
     if(n <= 64)
         return run_potrs_small<T, 64, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
-    if(n <= 64)
-        return run_potrs_nt<T, 64, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
     if(n <= 128)
         return run_potrs_nt<T, 128, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
     return run_potrs_nt<T, 256, NRC>(s, upper, n, nrhs, A, lda, B, ldb, skip, bc);
