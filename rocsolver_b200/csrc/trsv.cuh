@@ -436,8 +436,10 @@ __global__ void __launch_bounds__(N, N <= 32 ? 16 : 8)
     potrs_small_kernel(int upper, int n, int nrhs, Batch<T> A, int lda, Batch<T> B, int ldb,
                        const int* skip_info)
 {
-    constexpr int LD = N + 1;
-    __shared__ T sL[N * LD]; // L(r, c) at sL[r + c*LD], lower triangle
+    // the lower triangle packed by columns: L(i, j), i >= j, at sL[pk(j) + i - j] (half the
+    // shared memory of a square tile, so twice the members per SM)
+    __shared__ T sL[N * (N + 1) / 2];
+    auto pk = [](int j) { return (j * (2 * N - j + 1)) / 2; };
     __shared__ T sx[2][NRC];
     const int r = threadIdx.x;
     const int groups = (nrhs + NRC - 1) / NRC;
@@ -467,7 +469,7 @@ __global__ void __launch_bounds__(N, N <= 32 ? 16 : 8)
             const int e = e0 + u * N, p = e % N, q = e / N;
             const int i = upper ? q : p, j = upper ? p : q;
             if(e < N * N && i < n && j <= i)
-                sL[i + j * LD] = t[u];
+                sL[pk(j) + i - j] = t[u];
         }
     }
     T v[NRC];
@@ -475,7 +477,7 @@ __global__ void __launch_bounds__(N, N <= 32 ? 16 : 8)
     for(int k = 0; k < NRC; ++k)
         v[k] = (r < n && k < nc) ? x[ix(r, c0 + k, ldb)] : T(0);
     __syncthreads();
-    const T rd = r < n ? T(1) / sL[r + r * LD] : T(0);
+    const T rd = r < n ? T(1) / sL[pk(r)] : T(0);
     // forward: L y = b
 #pragma unroll 1
     for(int c = 0; c < n; ++c)
@@ -493,7 +495,7 @@ __global__ void __launch_bounds__(N, N <= 32 ? 16 : 8)
         __syncthreads();
         if(r > c && r < n)
         {
-            const T l = sL[r + c * LD];
+            const T l = sL[pk(c) + r - c];
 #pragma unroll
             for(int k = 0; k < NRC; ++k)
                 v[k] = fma(-l, sx[buf][k], v[k]);
@@ -516,7 +518,7 @@ __global__ void __launch_bounds__(N, N <= 32 ? 16 : 8)
         __syncthreads();
         if(r < c)
         {
-            const T l = sL[c + r * LD];
+            const T l = sL[pk(r) + c - r];
 #pragma unroll
             for(int k = 0; k < NRC; ++k)
                 v[k] = fma(-l, sx[buf][k], v[k]);
