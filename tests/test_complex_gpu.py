@@ -409,3 +409,22 @@ def test_kernel_boundaries(handle, P, n):
         oX = from_colmajor(oB, bc, n, nrhs, n, n * nrhs)
         for b in range(bc):
             assert norm_error("I", oX[b], X[b]) <= 20 * n * eps(P), (lower, b)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+@pytest.mark.parametrize("m,n", [(20, 7), (7, 20), (32, 32), (9, 16), (17, 5)])
+@pytest.mark.parametrize("pivot", [True, False])
+def test_warp_lu_small_shapes(handle, P, m, n, pivot):
+    """The one-warp-per-member LU (m, n <= 32): rectangular shapes, padded leading dimension,
+    with and without pivoting, against the oracle."""
+    A = uniform_complex(m, n, 5, seed=m * 31 + n).astype(DT[P])
+    if not pivot:
+        for b in range(5):
+            A[b][np.arange(min(m, n)), np.arange(min(m, n))] += 8.0
+    LU, ipiv, info = gpu_getrf(handle, P, A, pivot=pivot, lda=m + 2)
+    oLU, oipiv, oinfo = oracle_getrf(A, pivot=pivot)
+    np.testing.assert_array_equal(info, oinfo)
+    if pivot:
+        np.testing.assert_array_equal(ipiv, oipiv)
+    for b in range(5):
+        assert norm_error("F", oLU[b], LU[b]) <= 4 * max(m, n) * eps(P)
