@@ -6,14 +6,16 @@
 // (specialized/roclapack_trsm_specialized_kernels.hpp:219-380 conj_forward/backward
 // substitution) and Hermitian Cholesky (roclapack_potf2.hpp:185-248 with conjugated dots).
 //
-// Design: one CTA of CPX_NT threads per matrix, working in place in global memory (members
-// are L2-resident while their CTA runs).  getrf: per column a CTA-wide argmax of |re| + |im|
-// (LAPACK izamax: first index of the maximum, a NaN only wins in the first position, through
-// the same pivot keys as the real kernels), the row interchange over all columns, scaling by
-// the reciprocal (|pivot| >= sfmin) or by division, and the rank-1 update of the trailing
-// matrix spread over all threads (rows fastest: coalesced).  Solves sweep one unknown at a
-// time with the updates of the remaining rows spread over the threads.  These kernels favour
-// simplicity over speed: the tensor-core and register-resident kernels are FP32/FP64.
+// Design.  getrf: m, n <= 32 one warp per member with rows in registers
+// (cgetrf_warp_kernel); members up to 96 KB one CTA per member factoring a shared-memory copy
+// (cgetrf_smem_kernel); larger members the same device code in place in global memory
+// (cgetrf_kernel).  Per column: the pivot is the first largest |re| + |im| (LAPACK izamax; a
+// NaN only wins in the first position, through the same pivot keys as the real kernels), rows
+// are interchanged over all columns, the column is scaled by the reciprocal (|pivot| >=
+// sfmin) or by division, and the trailing matrix takes the rank-1 update.  potrf: the same
+// shared-memory / global split.  getrs and potrs for n <= 256: one warp per member and
+// right-hand side, no block barriers (cgetrs_warp_kernel, cpotrs_warp_kernel); larger n one
+// CTA per member sweeping one unknown at a time.
 #include "handle.h"
 #include "launch.h"
 #include "logger.h"
