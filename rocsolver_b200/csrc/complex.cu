@@ -525,6 +525,8 @@ __global__ void __launch_bounds__(CPX_NT)
 }
 
 // members of at most CPX_SMEM_MAX bytes: the referenced triangle is factored in shared memory
+// (larger members run cpotrf_kernel in place: after a failure their trailing part holds the
+// updates of the finished columns, as LAPACK's blocked zpotrf leaves its trailing blocks)
 template <typename C>
 __global__ void __launch_bounds__(CPX_NT)
     cpotrf_smem_kernel(int upper, int n, Batch<C> A, int lda, int* info)
@@ -539,9 +541,14 @@ __global__ void __launch_bounds__(CPX_NT)
             sa[i + (size_t)c * n] = RSB_AT(a, i, c, lda, n, n);
     __syncthreads();
     const int inf = cpotrf_dev<C>(upper, n, sa, n);
+    // write back what LAPACK zpotf2 leaves: everything, or after a failure at order k the
+    // finished columns (rows, for upper) before k and the failing pivot; the trailing part,
+    // updated here but not by zpotf2, keeps its input
+    const int k = inf ? inf - 1 : n;
     for(int c = warp; c < n; c += NW)
         for(int i = upper ? lane : c + lane; i < (upper ? c + 1 : n); i += 32)
-            RSB_AT(a, i, c, lda, n, n) = sa[i + (size_t)c * n];
+            if(min(i, c) < k || (i == k && c == k))
+                RSB_AT(a, i, c, lda, n, n) = sa[i + (size_t)c * n];
     if(threadIdx.x == 0)
         info[blockIdx.x] = inf;
 }

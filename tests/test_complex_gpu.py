@@ -428,3 +428,38 @@ def test_warp_lu_small_shapes(handle, P, m, n, pivot):
         np.testing.assert_array_equal(ipiv, oipiv)
     for b in range(5):
         assert norm_error("F", oLU[b], LU[b]) <= 4 * max(m, n) * eps(P)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+@pytest.mark.parametrize("n", [1, 5, 17, 32])
+@pytest.mark.parametrize("lower", [True, False])
+def test_warp_cholesky_small(handle, P, n, lower):
+    """Small Hermitian Cholesky (n <= 32, padded leading dimension): factors against the
+    oracle in the referenced triangle, the other triangle untouched, and a member that is not
+    positive definite (info, the failing pivot stored, later columns untouched)."""
+    bc = 4
+    A = hpd_gram(n, bc, seed=700 + n).astype(DT[P])
+    if n > 2:
+        A[2][n // 2, n // 2] = -1.0
+    C, info, _ = gpu_potrf(handle, P, A, lower, lda=n + 3)
+    oC = to_colmajor(A)
+    oI = np.zeros(bc, np.int32)
+    oracle.cpotrf(not lower, n, oC, n, n * n, oI, bc)
+    oCm = from_colmajor(oC, bc, n, n, n, n * n)
+    np.testing.assert_array_equal(info, oI)
+    f = norm_error_lower if lower else norm_error_upper
+    other = np.triu(np.ones((n, n), bool), 1) if lower else np.tril(np.ones((n, n), bool), -1)
+    for b in range(bc):
+        nn = n if info[b] == 0 else info[b] - 1
+        assert f("F", oCm[b][:nn, :nn], C[b][:nn, :nn]) <= n * eps(P)
+        np.testing.assert_array_equal(C[b][other], A[b][other])
+        if info[b] != 0:  # the failing pivot is stored; the columns after it keep A
+            k = info[b] - 1
+            assert abs(C[b][k, k] - oCm[b][k, k]) <= 1e3 * eps(P) * abs(oCm[b][k, k])
+            tail = np.tril(np.ones((n, n), bool), -1) if lower else np.triu(np.ones((n, n), bool), 1)
+            cols = np.zeros((n, n), bool)
+            if lower:
+                cols[:, k:] = True
+            else:
+                cols[k:, :] = True
+            np.testing.assert_array_equal(C[b][tail & cols], A[b][tail & cols])
