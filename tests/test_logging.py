@@ -130,3 +130,27 @@ def test_trace_kernels_and_profile_gpu(tmp_path, monkeypatch):
     assert "------- PROFILE -------" in text
     assert "rocsolver_getrf_template: Calls: 2, Total Time:" in text
     assert "    getrf_cta_kernel: Calls: 2, Total Time:" in text
+
+
+def test_complex_entry_points_log_their_precision(session):
+    """The c / z entry points log with -r c / -r z, as the reference's do
+    (rocsolver_logger.hpp get_precision for rocblas_float_complex / rocblas_double_complex),
+    with conjugate-transpose solves logged as --trans C."""
+    h = rs.Handle()
+    try:
+        st = rs.call("rocsolver_zgetrf_strided_batched", h.value, -1, 8, FAKE, 8, 64, FAKE, 8,
+                     FAKE, 2)
+        assert st == rs.INVALID_SIZE
+        st = rs.call("rocsolver_cgetrs_strided_batched", h.value, rs.OP_C, 8, 1, FAKE, 8, 64,
+                     FAKE, 8, FAKE, 8, 8, 0)
+        assert st == rs.SUCCESS
+        st = rs.call("rocsolver_zposv", h.value, rs.FILL_UPPER, -2, 1, FAKE, 1, FAKE, 1, FAKE)
+        assert st == rs.INVALID_SIZE
+    finally:
+        h.close()
+    assert rs.call("rocsolver_log_end") == rs.SUCCESS
+    lines = [l for l in session["bench"].read_text().splitlines()
+             if l.startswith("./rocsolver-bench")]
+    assert lines[0].startswith("./rocsolver-bench -f getrf_strided_batched -r z -m -1 -n 8")
+    assert lines[1].startswith("./rocsolver-bench -f getrs_strided_batched -r c --trans C")
+    assert lines[2].startswith("./rocsolver-bench -f posv -r z --uplo U -n -2")
