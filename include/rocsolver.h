@@ -1212,7 +1212,7 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_sgetri_npvt_outofplace_strided_batched
     rocblas_int* info,
     const rocblas_int batch_count);
 
-/* replaces lapack/roclapack_gesv_outofplace.cpp:106-135 (exported, not in the public header) */
+/* replaces lapack/roclapack_gesv_outofplace.cpp:106-119 (exported, not in the public header) */
 ROCSOLVER_EXPORT rocblas_status rocsolver_sgesv_outofplace(rocblas_handle handle,
     const rocblas_int n,
     const rocblas_int nrhs,
@@ -1345,7 +1345,7 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dgetri_npvt_outofplace_strided_batched
     rocblas_int* info,
     const rocblas_int batch_count);
 
-/* replaces lapack/roclapack_gesv_outofplace.cpp:106-135 (exported, not in the public header) */
+/* replaces lapack/roclapack_gesv_outofplace.cpp:121-135 (exported, not in the public header) */
 ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_outofplace(rocblas_handle handle,
     const rocblas_int n,
     const rocblas_int nrhs,
@@ -1355,6 +1355,273 @@ ROCSOLVER_EXPORT rocblas_status rocsolver_dgesv_outofplace(rocblas_handle handle
     double* B,
     const rocblas_int ldb,
     double* X,
+    const rocblas_int ldx,
+    rocblas_int* info);
+
+/* complex getri and gesv_outofplace: the same argument lists as the s / d forms above */
+/* replaces rocsolver-functions.h:9187 / lapack/roclapack_getri.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9263 / lapack/roclapack_getri_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9349 / lapack/roclapack_getri_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9414 / lapack/roclapack_getri.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_npvt(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9477 / lapack/roclapack_getri_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_npvt_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9548 / lapack/roclapack_getri_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_npvt_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21398 / lapack/roclapack_getri_outofplace.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_float_complex* C,
+    const rocblas_int ldc,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:21484 / lapack/roclapack_getri_outofplace_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_outofplace_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_float_complex* const C[],
+    const rocblas_int ldc,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21590 / lapack/roclapack_getri_outofplace_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_outofplace_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_float_complex* C,
+    const rocblas_int ldc,
+    const rocblas_stride strideC,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21669 / lapack/roclapack_getri_outofplace.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_npvt_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_float_complex* C,
+    const rocblas_int ldc,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:21744 / lapack/roclapack_getri_outofplace_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_npvt_outofplace_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* const A[],
+    const rocblas_int lda,
+    rocblas_float_complex* const C[],
+    const rocblas_int ldc,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21837 / lapack/roclapack_getri_outofplace_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgetri_npvt_outofplace_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_float_complex* C,
+    const rocblas_int ldc,
+    const rocblas_stride strideC,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces lapack/roclapack_gesv_outofplace.cpp:137-151 (exported, not in the public header) */
+ROCSOLVER_EXPORT rocblas_status rocsolver_cgesv_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_float_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_float_complex* B,
+    const rocblas_int ldb,
+    rocblas_float_complex* X,
+    const rocblas_int ldx,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9194 / lapack/roclapack_getri.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9272 / lapack/roclapack_getri_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9359 / lapack/roclapack_getri_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9420 / lapack/roclapack_getri.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_npvt(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:9484 / lapack/roclapack_getri_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_npvt_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:9556 / lapack/roclapack_getri_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_npvt_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21407 / lapack/roclapack_getri_outofplace.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_double_complex* C,
+    const rocblas_int ldc,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:21495 / lapack/roclapack_getri_outofplace_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_outofplace_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_double_complex* const C[],
+    const rocblas_int ldc,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21604 / lapack/roclapack_getri_outofplace_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_outofplace_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_int* ipiv,
+    const rocblas_stride strideP,
+    rocblas_double_complex* C,
+    const rocblas_int ldc,
+    const rocblas_stride strideC,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21677 / lapack/roclapack_getri_outofplace.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_npvt_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_double_complex* C,
+    const rocblas_int ldc,
+    rocblas_int* info);
+
+/* replaces rocsolver-functions.h:21754 / lapack/roclapack_getri_outofplace_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_npvt_outofplace_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* const A[],
+    const rocblas_int lda,
+    rocblas_double_complex* const C[],
+    const rocblas_int ldc,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces rocsolver-functions.h:21849 / lapack/roclapack_getri_outofplace_strided_batched.cpp */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgetri_npvt_outofplace_strided_batched(rocblas_handle handle,
+    const rocblas_int n,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    const rocblas_stride strideA,
+    rocblas_double_complex* C,
+    const rocblas_int ldc,
+    const rocblas_stride strideC,
+    rocblas_int* info,
+    const rocblas_int batch_count);
+
+/* replaces lapack/roclapack_gesv_outofplace.cpp:153-167 (exported, not in the public header) */
+ROCSOLVER_EXPORT rocblas_status rocsolver_zgesv_outofplace(rocblas_handle handle,
+    const rocblas_int n,
+    const rocblas_int nrhs,
+    rocblas_double_complex* A,
+    const rocblas_int lda,
+    rocblas_int* ipiv,
+    rocblas_double_complex* B,
+    const rocblas_int ldb,
+    rocblas_double_complex* X,
     const rocblas_int ldx,
     rocblas_int* info);
 

@@ -94,7 +94,7 @@ def getri(n, A, lda, strideA, ipiv, strideP, info, bc, pivot=True, nthreads=1):
 
 
 # ---- complex (c/z): complex64 / complex128 numpy buffers; op 0 getrf, 1 getrs (trans 0 N,
-# 1 T, 2 C), 2 potrf, 3 potrs, 4 gesv, 5 posv (oracle/oracle_complex.c)
+# 1 T, 2 C), 2 potrf, 3 potrs, 4 gesv, 5 posv, 6 getri (oracle/oracle_complex.c)
 def _cbatch(op, A, m=0, n=0, nrhs=0, trans=0, upper=0, pivot=1, lda=1, sA=0, ipiv=None, sP=0,
             B=None, ldb=1, sB=0, info=None, bc=1):
     l = lib()
@@ -134,6 +134,11 @@ def cgesv(n, nrhs, A, lda, strideA, ipiv, strideP, B, ldb, strideB, info, bc):
 
 def cposv(upper, n, nrhs, A, lda, strideA, B, ldb, strideB, info, bc):
     _cbatch(5, A, n, n, nrhs, 0, int(upper), 0, lda, strideA, None, 0, B, ldb, strideB, info, bc)
+
+
+def cgetri(n, A, lda, strideA, ipiv, strideP, info, bc, pivot=True):
+    """Inverse from the LU factors (LAPACK zgetri / cgetri); A overwritten where info == 0."""
+    _cbatch(6, A, n, n, 0, 0, 0, int(pivot), lda, strideA, ipiv, strideP, None, 1, 0, info, bc)
 
 
 def refgen(count):

@@ -16,6 +16,7 @@
  *            j with ajj <= 0 or NaN (a_jj set to ajj, then stop)
  *   zpotrs : lower L Y = B, L^H X = Y; upper U^H Y = B, U X = Y
  *   gesv / posv: B left unchanged where info > 0
+ *   zgetri : inverse from the LU factors (ztrti2 + unblocked zgetri, as oracle.c's dgetri)
  * Pinned against scipy's bundled OpenBLAS LAPACK by tests/golden/make_golden.py.
  * Arrays are interleaved (re, im) pairs, column-major, member b at A + b*strideA elements.
  */
@@ -24,6 +25,7 @@
 #include <math.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #define IDX(i, j, ld) ((size_t)(i) + (size_t)(j) * (size_t)(ld))
 
@@ -193,7 +195,66 @@
             P##_trsv(n, nrhs, A, lda, B, ldb, 1, 1, 1, 0);                                   \
         }                                                                                    \
     }                                                                                        \
-    /* batch driver: op 0 getrf, 1 getrs, 2 potrf, 3 potrs, 4 gesv, 5 posv */               \
+    /* inverse from the LU factors (LAPACK zgetri unblocked, as oracle.c's dgetri): info =  \
+       first zero U(i,i) with A untouched; inv(U) by ztrti2; X L = inv(U) from the right;    \
+       column interchanges in reverse order (none when pivot = 0) */                          \
+    static void P##_getri(int n, C* A, int lda, const int* ipiv, int* info, int pivot)       \
+    {                                                                                        \
+        *info = 0;                                                                           \
+        for(int i = 0; i < n; ++i)                                                           \
+            if(A[IDX(i, i, lda)] == (C)0)                                                    \
+            {                                                                                \
+                *info = i + 1;                                                               \
+                return;                                                                      \
+            }                                                                                \
+        for(int j = 0; j < n; ++j)                                                           \
+        {                                                                                    \
+            A[IDX(j, j, lda)] = (C)1 / A[IDX(j, j, lda)];                                    \
+            C ajj = -A[IDX(j, j, lda)];                                                      \
+            for(int jj = 0; jj < j; ++jj)                                                    \
+            {                                                                                \
+                C t = A[IDX(jj, j, lda)];                                                    \
+                if(t != (C)0)                                                                \
+                {                                                                            \
+                    for(int i = 0; i < jj; ++i)                                              \
+                        A[IDX(i, j, lda)] += t * A[IDX(i, jj, lda)];                         \
+                    A[IDX(jj, j, lda)] = t * A[IDX(jj, jj, lda)];                            \
+                }                                                                            \
+            }                                                                                \
+            for(int i = 0; i < j; ++i)                                                       \
+                A[IDX(i, j, lda)] *= ajj;                                                    \
+        }                                                                                    \
+        C* work = (C*)malloc(sizeof(C) * (size_t)(n > 0 ? n : 1));                           \
+        for(int j = n - 1; j >= 0; --j)                                                      \
+        {                                                                                    \
+            for(int i = j + 1; i < n; ++i)                                                   \
+            {                                                                                \
+                work[i] = A[IDX(i, j, lda)];                                                 \
+                A[IDX(i, j, lda)] = (C)0;                                                    \
+            }                                                                                \
+            for(int jj = j + 1; jj < n; ++jj)                                                \
+            {                                                                                \
+                C t = -work[jj];                                                             \
+                if(t != (C)0)                                                                \
+                    for(int i = 0; i < n; ++i)                                               \
+                        A[IDX(i, j, lda)] += t * A[IDX(i, jj, lda)];                         \
+            }                                                                                \
+        }                                                                                    \
+        free(work);                                                                          \
+        if(pivot)                                                                            \
+            for(int j = n - 2; j >= 0; --j)                                                  \
+            {                                                                                \
+                int jp = ipiv[j] - 1;                                                        \
+                if(jp != j)                                                                  \
+                    for(int i = 0; i < n; ++i)                                               \
+                    {                                                                        \
+                        C t = A[IDX(i, j, lda)];                                             \
+                        A[IDX(i, j, lda)] = A[IDX(i, jp, lda)];                              \
+                        A[IDX(i, jp, lda)] = t;                                              \
+                    }                                                                        \
+            }                                                                                \
+    }                                                                                        \
+    /* batch driver: op 0 getrf, 1 getrs, 2 potrf, 3 potrs, 4 gesv, 5 posv, 6 getri */       \
     void oracle_##P##batch(int op, int m, int n, int nrhs, int trans, int upper, int pivot,  \
                            C* A, int lda, int64_t sA, int* ipiv, int64_t sP, C* B, int ldb,  \
                            int64_t sB, int* info, int bc)                                    \
@@ -221,6 +282,7 @@
                 if(*inf == 0)                                                                \
                     P##_potrs(upper, n, nrhs, a, lda, x, ldb);                               \
                 break;                                                                       \
+            case 6: P##_getri(n, a, lda, p, inf, pivot); break;                              \
             }                                                                                \
         }                                                                                    \
     }

@@ -78,9 +78,8 @@ _SIG = {
     "gesv_outofplace": [I, I, P, I, P, P, I, P, I, P],
 }
 
-# families the complex precisions (c, z) export: the factor-and-solve ones
-_COMPLEX_FAMILIES = [f for f in _SIG if f.startswith(("getrf", "getrs", "gesv", "potr", "posv"))
-                     and f != "gesv_outofplace"]
+# families the complex precisions (c, z) export: all of them
+_COMPLEX_FAMILIES = list(_SIG)
 
 # entry points with no counterpart in the reference (declared in include/rocsolver.h)
 _EXTRA = {

@@ -204,7 +204,7 @@ rocblas_status getri_impl(rocblas_handle h, int n, Batch<T> A, const void* Aptr,
         return rocblas_status_invalid_handle;
     if(n < 0 || lda < n || (outofplace && ldc < n) || bc < 0)
         return rocblas_status_invalid_size;
-    const size_t ws_bytes = (n && bc) ? getri_workspace(n, bc, sizeof(T), !outofplace) : 0;
+    const size_t ws_bytes = (n && bc) ? getri_workspace<T>(n, bc, !outofplace) : 0;
     if(h->querying)
         return ws_query(h, ws_bytes);
     if((n && !Aptr) || (outofplace && n && !Cptr) || (n && pivot && !ipiv) || (bc && !info))
@@ -743,4 +743,6 @@ RSB_API_TYPE(c, rocblas_float_complex)
 RSB_API_TYPE(z, rocblas_double_complex)
 RSB_API_GETRI(s, float)
 RSB_API_GETRI(d, double)
+RSB_API_GETRI(c, rocblas_float_complex)
+RSB_API_GETRI(z, rocblas_double_complex)
 }

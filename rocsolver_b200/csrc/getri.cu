@@ -22,6 +22,32 @@
 
 namespace rsb {
 
+// 0, 1 and the zero test for the real and the complex element types
+template <typename T>
+struct GetriNum
+{
+    static constexpr bool complex_type = false;
+    static __device__ T zero() { return T(0); }
+    static __device__ T one() { return T(1); }
+    static __device__ bool is_zero(T x) { return x == T(0); }
+};
+template <typename C>
+struct GetriNumC
+{
+    static constexpr bool complex_type = true;
+    static __device__ C zero() { C z; z.x = 0; z.y = 0; return z; }
+    static __device__ C one() { C z; z.x = 1; z.y = 0; return z; }
+    static __device__ bool is_zero(C x) { return x.x == 0 && x.y == 0; }
+};
+template <>
+struct GetriNum<rocblas_float_complex> : GetriNumC<rocblas_float_complex>
+{
+};
+template <>
+struct GetriNum<rocblas_double_complex> : GetriNumC<rocblas_double_complex>
+{
+};
+
 // info[b] = first i (1-based) with U(i,i) == 0, else 0; W_b = I (n x n, ld ldw).  One CTA
 // per member.
 template <typename T>
@@ -37,7 +63,7 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     int mine = INT_MAX;
     for(int i = threadIdx.x; i < n; i += blockDim.x)
-        if(a[ix(i, i, lda)] == T(0))
+        if(GetriNum<T>::is_zero(a[ix(i, i, lda)]))
         {
             mine = i;
             break;
@@ -48,7 +74,7 @@ __global__ void __launch_bounds__(256)
     for(int64_t e = threadIdx.x; e < total; e += blockDim.x)
     {
         const int i = (int)(e % n), j = (int)(e / n);
-        w[ix(i, j, ldw)] = i == j ? T(1) : T(0);
+        w[ix(i, j, ldw)] = i == j ? GetriNum<T>::one() : GetriNum<T>::zero();
     }
     __syncthreads();
     if(threadIdx.x == 0)
@@ -82,7 +108,7 @@ constexpr int GETRI_SMALL_BYTES = 64 * 1024;
 template <typename T>
 static bool getri_small(int n)
 {
-    return n <= 128 && (size_t)n * n * sizeof(T) <= GETRI_SMALL_BYTES;
+    return !GetriNum<T>::complex_type && n <= 128 && (size_t)n * n * sizeof(T) <= GETRI_SMALL_BYTES;
 }
 
 // C.base == C.ptrs == nullptr: the inverse overwrites A.  Members whose U has a zero diagonal
@@ -174,16 +200,17 @@ __global__ void __launch_bounds__(NT)
         info[b] = 0;
 }
 
-size_t getri_workspace(int n, int bc, size_t elem, bool inplace)
+template <typename T>
+size_t getri_workspace(int n, int bc, bool inplace)
 {
-    const bool small = elem == sizeof(double) ? getri_small<double>(n) : getri_small<float>(n);
-    return inplace && !small ? ws_round(elem * (size_t)n * n * bc) : 0;
+    return inplace && !getri_small<T>(n) ? ws_round(sizeof(T) * (size_t)n * n * bc) : 0;
 }
 
 template <typename T>
 rocblas_status launch_getri(cudaStream_t s, int n, Batch<T> A, int lda, const int* ipiv,
                             int64_t strideP, Batch<T> C, int ldc, int* info, int bc, void* ws)
 {
+    if constexpr(!GetriNum<T>::complex_type)
     if(getri_small<T>(n))
     {
         const size_t smem = sizeof(T) * (size_t)n * n;
@@ -219,7 +246,11 @@ rocblas_status launch_getri(cudaStream_t s, int n, Batch<T> A, int lda, const in
     }
     if(cudaGetLastError() != cudaSuccess)
         return rocblas_status_internal_error;
-    rocblas_status st = launch_getrs_many<T>(s, n, n, A, lda, ipiv, strideP, W, ldw, info, bc);
+    rocblas_status st;
+    if constexpr(GetriNum<T>::complex_type)
+        st = launch_getrs<T>(s, 0, n, n, A, lda, ipiv, strideP, W, ldw, info, bc, no_gate());
+    else
+        st = launch_getrs_many<T>(s, n, n, A, lda, ipiv, strideP, W, ldw, info, bc);
     if(st != rocblas_status_success || !inplace)
         return st;
     RSB_LOG_KERNEL("getri_copy_back_kernel");
@@ -228,9 +259,13 @@ rocblas_status launch_getri(cudaStream_t s, int n, Batch<T> A, int lda, const in
                                              : rocblas_status_internal_error;
 }
 
-template rocblas_status launch_getri<float>(cudaStream_t, int, Batch<float>, int, const int*,
-                                            int64_t, Batch<float>, int, int*, int, void*);
-template rocblas_status launch_getri<double>(cudaStream_t, int, Batch<double>, int, const int*,
-                                             int64_t, Batch<double>, int, int*, int, void*);
+#define RSB_GETRI_INST(T)                                                                    \
+    template size_t getri_workspace<T>(int, int, bool);                                      \
+    template rocblas_status launch_getri<T>(cudaStream_t, int, Batch<T>, int, const int*,     \
+                                            int64_t, Batch<T>, int, int*, int, void*);
+RSB_GETRI_INST(float)
+RSB_GETRI_INST(double)
+RSB_GETRI_INST(rocblas_float_complex)
+RSB_GETRI_INST(rocblas_double_complex)
 
 } // namespace rsb

@@ -60,7 +60,8 @@ RSB_DECLARE_COMPLEX_LAUNCHERS(rocblas_double_complex)
 // inverse from the LU factors (getri.cu): C.base == C.ptrs == nullptr means in place (the
 // inverse is formed in ws, getri_workspace bytes, and copied over A where info == 0);
 // ipiv == nullptr means no pivoting (npvt forms)
-size_t getri_workspace(int n, int bc, size_t elem, bool inplace);
+template <typename T>
+size_t getri_workspace(int n, int bc, bool inplace);
 template <typename T>
 rocblas_status launch_getri(cudaStream_t s, int n, Batch<T> A, int lda, const int* ipiv,
                             int64_t strideP, Batch<T> C, int ldc, int* info, int bc, void* ws);

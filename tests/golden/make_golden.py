@@ -284,6 +284,29 @@ def main_complex():
                     pivs.append((piv + 1).astype(np.int32)); xs.append(x); infos.append(int(info))
                 put(f"{P}gesv_ref_n{n}_r{nrhs}_s{int(singular)}", ipiv=np.stack(pivs),
                     X=np.stack(xs), info=np.array(infos, np.int32))
+    # getri (zgetri / cgetri) on the reference's getri inputs, zeroed U diagonal entries in
+    # the singular members
+    for P, cdt, sizes in (("z", np.complex128, ((32, False), (50, True))),
+                          ("c", np.complex64, ((32, False),))):
+        getrf, getri = getattr(la, P + "getrf"), getattr(la, P + "getri")
+        for n, singular in sizes:
+            A = ref_getri_matrix(n, n, BC, cplx=True).astype(cdt)
+            lus, pivs, invs, infos = [], [], [], []
+            for b in range(BC):
+                lu, piv, info = getrf(A[b], overwrite_a=0)
+                assert info == 0
+                if singular:
+                    for i in ref_getri_singular(b, BC, n):
+                        lu[i, i] = 0.0
+                inv, info2 = getri(lu, piv)
+                lus.append(lu); pivs.append((piv + 1).astype(np.int32)); infos.append(int(info2))
+                invs.append(inv if info2 == 0 else lu)
+            key = f"{P}getri_ref_n{n}_s{int(singular)}"
+            out[key + "_LU"] = np.stack(lus)
+            out[key + "_ipiv"] = np.stack(pivs)
+            out[key + "_inv"] = np.stack(invs)
+            out[key + "_info"] = np.array(infos, np.int32)
+            cases.append(key)
     out["cases"] = np.array(cases)
     path = os.path.join(HERE, "lapack_golden_complex.npz")
     np.savez_compressed(path, **out)

@@ -77,10 +77,11 @@ def ref_potrf_input(n, bc, singular, cplx=False):
     return A
 
 
-def ref_getri_matrix(n, lda, bc):
+def ref_getri_matrix(n, lda, bc, cplx=False):
     """clients/include/testing_getri.hpp:102-150 before its host getrf: integers 1..10 scaled
-    to v/10 + 10 on the diagonal and (v - 4)/10 off it, rows reversed."""
-    A = _member_view(_refstream(bc * lda * n), bc, lda, n)[:, :n, :].copy()
+    to v/10 + 10 on the diagonal and (v - 4)/10 off it, rows reversed (complex: the shifts
+    act on the real part)."""
+    A = _member_view(_refstream(bc * lda * n, cplx), bc, lda, n)[:, :n, :].copy()
     idx = np.arange(n)
     for b in range(bc):
         M = (A[b] - 4.0) / 10.0

@@ -165,7 +165,7 @@ def test_potrf_potrs_posv_bad_args(handle, p):
     assert rs.call(v, handle, rs.FILL_LOWER, 1, 1, FAKE, 1, 1, FAKE, 1, 1, NULL, 0) == rs.SUCCESS
 
 
-@pytest.mark.parametrize("p", ["s", "d"])
+@pytest.mark.parametrize("p", ["s", "d", "c", "z"])
 def test_getri_bad_args(handle, p):
     """clients/include/testing_getri.hpp:15-88 and testing_getri_outofplace.hpp bad-arg
     order: handle, sizes (n, lda, ldc, bc), then pointers (A, C, ipiv unless npvt, info)."""
@@ -200,10 +200,10 @@ def test_getri_bad_args(handle, p):
     assert c(n=200, lda=200, sA=40000, sP=200, bc=10) == rs.SIZE_INCREASED
     assert rs.call("rocblas_stop_device_memory_size_query", handle, ctypes.byref(sz)) \
         == rs.SUCCESS
-    assert sz.value >= 200 * 200 * 10 * (8 if p == "d" else 4)
+    assert sz.value >= 200 * 200 * 10 * {"s": 4, "d": 8, "c": 8, "z": 16}[p]
 
 
-@pytest.mark.parametrize("p", ["s", "d"])
+@pytest.mark.parametrize("p", ["s", "d", "c", "z"])
 def test_gesv_outofplace_bad_args(handle, p):
     """clients/include/testing_gesv_outofplace.hpp:15-90 bad-arg order."""
     f = f"rocsolver_{p}gesv_outofplace"

@@ -463,3 +463,89 @@ def test_warp_cholesky_small(handle, P, n, lower):
             else:
                 cols[k:, :] = True
             np.testing.assert_array_equal(C[b][tail & cols], A[b][tail & cols])
+
+
+# ---------------------------------------------------------------- getri and gesv_outofplace
+@pytest.mark.parametrize("key", [c for c in [str(x) for x in GOLD["cases"]]
+                                 if c[1:].startswith("getri")])
+@pytest.mark.parametrize("form", ["strided", "batched", "outofplace"])
+def test_getri_reference_inputs(handle, key, form):
+    """c / z getri from the golden LAPACK factors: info exact, inverse within n*eps (F-norm);
+    singular members keep their factors (getri_outofplace: C = I, as the real path)."""
+    P = key[0]
+    n = int(key.split("_n")[1].split("_")[0])
+    LU = GOLD[key + "_LU"].astype(DT[P])
+    ipiv = GOLD[key + "_ipiv"].astype(np.int32).reshape(-1).copy()
+    dA = dev(to_colmajor(LU, n + 1))
+    dP = dev(ipiv)
+    dI = dev(np.full(3, -7, np.int32))
+    lda = n + 1
+    if form == "strided":
+        _call(f"rocsolver_{P}getri_strided_batched", handle, n, ptr(dA), lda, lda * n, ptr(dP), n,
+              ptr(dI), 3)
+        out = from_colmajor(host(dA), 3, n, n, lda, lda * n)
+    elif form == "batched":
+        aA = ptr_array(dA, 3, lda * n)
+        _call(f"rocsolver_{P}getri_batched", handle, n, ptr(aA), lda, ptr(dP), n, ptr(dI), 3)
+        out = from_colmajor(host(dA), 3, n, n, lda, lda * n)
+    else:
+        dC = dev(np.zeros(3 * n * n, DT[P]))
+        _call(f"rocsolver_{P}getri_outofplace_strided_batched", handle, n, ptr(dA), lda, lda * n,
+              ptr(dP), n, ptr(dC), n, n * n, ptr(dI), 3)
+        out = from_colmajor(host(dC), 3, n, n, n, n * n)
+    info = host(dI)
+    np.testing.assert_array_equal(info, GOLD[key + "_info"])
+    for b in range(3):
+        if info[b] == 0:
+            assert norm_error("F", GOLD[key + "_inv"][b], out[b]) <= 4 * n * eps(P)
+        elif form == "outofplace":
+            np.testing.assert_array_equal(out[b], np.eye(n))
+        else:
+            np.testing.assert_array_equal(out[b], LU[b])
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+@pytest.mark.parametrize("n", [1, 7, 32, 33, 100, 256, 300])
+@pytest.mark.parametrize("pivot", [True, False])
+def test_getri_vs_oracle(handle, P, n, pivot):
+    """c / z getri (in place, with and without pivoting) against the complex oracle."""
+    A = (uniform_complex(n, n, 2, seed=4200 + n) + 2 * n * np.eye(n)[None]).astype(DT[P])
+    LU, ipiv, info = gpu_getrf(handle, P, A, pivot=pivot)
+    assert not info.any()
+    f = to_colmajor(LU)
+    fP = ipiv.reshape(-1).astype(np.int32).copy()
+    oI = np.zeros(2, np.int32)
+    oracle.cgetri(n, f, n, n * n, fP, n, oI, 2, pivot=pivot)
+    ref = from_colmajor(f, 2, n, n, n, n * n)
+    dA, dI, dP = dev(to_colmajor(LU)), dev(np.full(2, -7, np.int32)), dev(fP)
+    if pivot:
+        _call(f"rocsolver_{P}getri_strided_batched", handle, n, ptr(dA), n, n * n, ptr(dP), n,
+              ptr(dI), 2)
+    else:
+        _call(f"rocsolver_{P}getri_npvt_strided_batched", handle, n, ptr(dA), n, n * n, ptr(dI),
+              2)
+    np.testing.assert_array_equal(host(dI), oI)
+    inv = from_colmajor(host(dA), 2, n, n, n, n * n)
+    for b in range(2):
+        assert norm_error("F", ref[b], inv[b]) <= 8 * n * eps(P)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+@pytest.mark.parametrize("n", [5, 32, 64])
+def test_gesv_outofplace(handle, P, n):
+    """X = A^{-1} B with B left as it was; A and ipiv hold the factors (zgesv's)."""
+    nrhs = 3
+    A = uniform_complex(n, n, 1, seed=77 + n).astype(DT[P])
+    B = uniform_complex(n, nrhs, 1, seed=78 + n).astype(DT[P])
+    oA, oB = to_colmajor(A), to_colmajor(B)
+    oP, oI = np.zeros(n, np.int32), np.zeros(1, np.int32)
+    oracle.cgesv(n, nrhs, oA, n, n * n, oP, n, oB, n, n * nrhs, oI, 1)
+    dA, dB, dX = dev(to_colmajor(A)), dev(to_colmajor(B)), dev(np.zeros(n * nrhs, DT[P]))
+    dP, dI = dev(np.zeros(n, np.int32)), dev(np.full(1, -7, np.int32))
+    _call(f"rocsolver_{P}gesv_outofplace", handle, n, nrhs, ptr(dA), n, ptr(dP), ptr(dB), n,
+          ptr(dX), n, ptr(dI))
+    assert host(dI)[0] == 0
+    np.testing.assert_array_equal(host(dP), oP)
+    np.testing.assert_array_equal(host(dB), to_colmajor(B))
+    X = from_colmajor(host(dX), 1, n, nrhs, n, n * nrhs)[0]
+    assert norm_error("I", from_colmajor(oB, 1, n, nrhs, n, n * nrhs)[0], X) <= 20 * n * eps(P)

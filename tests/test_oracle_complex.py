@@ -130,3 +130,23 @@ def test_complex_reference_stream_pairs():
     z = _refstream(10, cplx=True)
     np.testing.assert_array_equal(z.real, v[0::2])
     np.testing.assert_array_equal(z.imag, v[1::2])
+
+
+@pytest.mark.parametrize("key", [c for c in CASES if c[1:].startswith("getri")])
+def test_complex_oracle_getri_matches_lapack(key):
+    """zgetri / cgetri from the golden factors: info exact, inverse within n*eps (F-norm,
+    relative); singular members keep their factors."""
+    P, _, _, kv = _parse(key)
+    n = kv["n"]
+    LU = GOLD[key + "_LU"]
+    f = to_colmajor(LU)
+    ipiv = GOLD[key + "_ipiv"].astype(np.int32).reshape(-1).copy()
+    info = np.zeros(3, np.int32)
+    oracle.cgetri(n, f, n, n * n, ipiv, n, info, 3)
+    inv = from_colmajor(f, 3, n, n, n, n * n)
+    np.testing.assert_array_equal(info, GOLD[key + "_info"])
+    for b in range(3):
+        if info[b] == 0:
+            assert norm_error("F", GOLD[key + "_inv"][b], inv[b]) <= n * _eps(P)
+        else:
+            np.testing.assert_array_equal(inv[b], LU[b])
