@@ -6,11 +6,11 @@
 // roclapack_getri_outofplace.hpp:73-127 (check_singularity, C = I, getrs on C).
 //
 // B200 design: orders whose member fits in 64 KB of shared memory (FP64 n <= 90, FP32
-// n <= 128) are inverted on chip by one CTA per member with LAPACK's own unblocked steps
-// (getri_small_kernel: one pass over the factors in, one over the inverse out).  Larger
-// orders solve A C = I with the library's getrs kernels (one warp per
-// matrix and right-hand-side group for n <= 32, otherwise one CTA per matrix and group of
-// four columns, the factors staged through inverted diagonal blocks), after one prep kernel
+// n <= 128, complex double n <= 64, complex float n <= 90) are inverted on chip by one CTA
+// per member with LAPACK's own unblocked steps (getri_small_kernel: one pass over the
+// factors in, one over the inverse out).  Larger orders solve A C = I with the library's
+// getrs kernels (one warp per matrix and right-hand-side group for n <= 32, otherwise one
+// CTA per matrix and group of right-hand sides), after one prep kernel
 // that finds the first zero diagonal entry of U (info, LAPACK dtrtri's singularity test) and
 // writes the identity into C.  In-place getri solves into the handle workspace and copies
 // the inverse back over the factors of the members with info = 0; members with info > 0 keep
@@ -30,14 +30,41 @@ struct GetriNum
     static __device__ T zero() { return T(0); }
     static __device__ T one() { return T(1); }
     static __device__ bool is_zero(T x) { return x == T(0); }
+    static __device__ T add(T a, T b) { return a + b; }
+    static __device__ T sub(T a, T b) { return a - b; }
+    static __device__ T mul(T a, T b) { return a * b; }
+    static __device__ T neg(T a) { return -a; }
+    static __device__ T inv(T a) { return T(1) / a; }
 };
 template <typename C>
 struct GetriNumC
 {
     static constexpr bool complex_type = true;
-    static __device__ C zero() { C z; z.x = 0; z.y = 0; return z; }
-    static __device__ C one() { C z; z.x = 1; z.y = 0; return z; }
+    static __device__ C mk(double re, double im)
+    {
+        C z;
+        z.x = re;
+        z.y = im;
+        return z;
+    }
+    static __device__ C zero() { return mk(0, 0); }
+    static __device__ C one() { return mk(1, 0); }
     static __device__ bool is_zero(C x) { return x.x == 0 && x.y == 0; }
+    static __device__ C add(C a, C b) { return mk(a.x + b.x, a.y + b.y); }
+    static __device__ C sub(C a, C b) { return mk(a.x - b.x, a.y - b.y); }
+    static __device__ C mul(C a, C b) { return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+    static __device__ C neg(C a) { return mk(-a.x, -a.y); }
+    // 1 / a by Smith's method (scaled by the larger component)
+    static __device__ C inv(C a)
+    {
+        if(fabs(a.x) >= fabs(a.y))
+        {
+            const auto r = a.y / a.x, d = a.x + a.y * r;
+            return mk(1 / d, -r / d);
+        }
+        const auto r = a.x / a.y, d = a.y + a.x * r;
+        return mk(r / d, -1 / d);
+    }
 };
 template <>
 struct GetriNum<rocblas_float_complex> : GetriNumC<rocblas_float_complex>
@@ -108,7 +135,7 @@ constexpr int GETRI_SMALL_BYTES = 64 * 1024;
 template <typename T>
 static bool getri_small(int n)
 {
-    return !GetriNum<T>::complex_type && n <= 128 && (size_t)n * n * sizeof(T) <= GETRI_SMALL_BYTES;
+    return n <= 128 && (size_t)n * n * sizeof(T) <= GETRI_SMALL_BYTES;
 }
 
 // C.base == C.ptrs == nullptr: the inverse overwrites A.  Members whose U has a zero diagonal
@@ -134,7 +161,7 @@ __global__ void __launch_bounds__(NT)
     {
         for(int c = 0; c < n; ++c)
             s[i + c * n] = RSB_AT(a, i, c, lda, n, n);
-        if(s[i + i * n] == T(0))
+        if(GetriNum<T>::is_zero(s[i + i * n]))
             atomicMin(&first, i);
     }
     __syncthreads();
@@ -142,7 +169,7 @@ __global__ void __launch_bounds__(NT)
     {
         if(!inplace && i < n)
             for(int c = 0; c < n; ++c)
-                RSB_AT(out, i, c, ldo, n, n) = i == c ? T(1) : T(0);
+                RSB_AT(out, i, c, ldo, n, n) = i == c ? GetriNum<T>::one() : GetriNum<T>::zero();
         if(i == 0)
             info[b] = first + 1;
         return;
@@ -151,28 +178,28 @@ __global__ void __launch_bounds__(NT)
     for(int j = 0; j < n; ++j)
     {
         if(i == j)
-            s[j + j * n] = T(1) / s[j + j * n];
+            s[j + j * n] = GetriNum<T>::inv(s[j + j * n]);
         __syncthreads();
-        T t = T(0);
+        T t = GetriNum<T>::zero();
         if(i < j)
             for(int k = i; k < j; ++k)
-                t += s[i + k * n] * s[k + j * n];
-        const T ajj = -s[j + j * n];
+                t = GetriNum<T>::add(t, GetriNum<T>::mul(s[i + k * n], s[k + j * n]));
+        const T ajj = GetriNum<T>::neg(s[j + j * n]);
         __syncthreads();
         if(i < j)
-            s[i + j * n] = t * ajj;
+            s[i + j * n] = GetriNum<T>::mul(t, ajj);
     }
     __syncthreads();
     // X L = inv(U), columns from the right: X(:, j) -= X(:, j+1:n) L(j+1:n, j), L(:, j) -> 0
     for(int j = n - 2; j >= 0; --j)
     {
-        T t = T(0);
+        T t = GetriNum<T>::zero();
         if(i < n)
             for(int k = j + 1; k < n; ++k)
-                t += s[i + k * n] * s[k + j * n];
+                t = GetriNum<T>::add(t, GetriNum<T>::mul(s[i + k * n], s[k + j * n]));
         __syncthreads();
         if(i < n)
-            s[i + j * n] = (i > j ? T(0) : s[i + j * n]) - t;
+            s[i + j * n] = GetriNum<T>::sub(i > j ? GetriNum<T>::zero() : s[i + j * n], t);
         __syncthreads();
     }
     // column interchanges in reverse order, each thread on its own row
@@ -210,7 +237,6 @@ template <typename T>
 rocblas_status launch_getri(cudaStream_t s, int n, Batch<T> A, int lda, const int* ipiv,
                             int64_t strideP, Batch<T> C, int ldc, int* info, int bc, void* ws)
 {
-    if constexpr(!GetriNum<T>::complex_type)
     if(getri_small<T>(n))
     {
         const size_t smem = sizeof(T) * (size_t)n * n;
