@@ -80,13 +80,45 @@ __device__ __forceinline__ C cdiv(C a, C b)
     return cx<C>((a.x * r + a.y) / d, (a.y * r - a.x) / d);
 }
 
-// 1 / z for |z| >= sfmin with one real division: z scaled by the power of two 2^-e of its
-// larger component (exact), 1/z = conj(z') / |z'|^2 * 2^-e
+// larger components between which |z|^2 neither overflows nor underflows
+template <typename R>
+struct CxSafe;
+template <>
+struct CxSafe<double>
+{
+    static __device__ __forceinline__ double lo() { return 0x1p-500; }
+    static __device__ __forceinline__ double hi() { return 0x1p+500; }
+};
+template <>
+struct CxSafe<float>
+{
+    static __device__ __forceinline__ float lo() { return 0x1p-60f; }
+    static __device__ __forceinline__ float hi() { return 0x1p+60f; }
+};
+
+// |z| >= sfmin (LAPACK zgetf2's test on the pivot's modulus): the larger component decides
+// it without a square root unless z is tiny
+template <typename C>
+__device__ __forceinline__ bool cbig(C z)
+{
+    using R = typename CxReal<C>::R;
+    return fmax(fabs(z.x), fabs(z.y)) >= Lim<R>::sfmin() || hypot(z.x, z.y) >= Lim<R>::sfmin();
+}
+
+// 1 / z for |z| >= sfmin with one real reciprocal: 1/z = conj(z) / |z|^2 while the larger
+// component lies in the safe range; otherwise z is first scaled by the power of two 2^-e of
+// its larger component (exact), 1/z = conj(z') / |z'|^2 * 2^-e
 template <typename C>
 __device__ __forceinline__ C crcp(C z)
 {
     using R = typename CxReal<C>::R;
-    const int e = ilogb(fmax(fabs(z.x), fabs(z.y)));
+    const R mx = fmax(fabs(z.x), fabs(z.y));
+    if(mx >= CxSafe<R>::lo() && mx <= CxSafe<R>::hi())
+    {
+        const R inv = Lim<R>::rcp(z.x * z.x + z.y * z.y);
+        return cx<C>(z.x * inv, -z.y * inv);
+    }
+    const int e = ilogb(mx);
     const R x = scalbn(z.x, -e), y = scalbn(z.y, -e);
     const R inv = R(1) / (x * x + y * y);
     return cx<C>(scalbn(x * inv, -e), scalbn(-y * inv, -e));
@@ -184,7 +216,7 @@ __device__ __forceinline__ int cgetrf_dev(int m, int n, C* a, int lda, int* piv,
                     }
             if(j + 1 + tid < m) // only threads with a row to scale form the reciprocal
             {
-                const bool recip = hypot(pv.x, pv.y) >= Lim<R>::sfmin();
+                const bool recip = cbig(pv);
                 const C r = recip ? crcp(pv) : pv;
                 for(int i = j + 1 + tid; i < m; i += CPX_NT)
                 {
@@ -265,7 +297,7 @@ __global__ void __launch_bounds__(32 * CPX_WPB)
         C* row = srow[warp][buf];
         // this lane's candidate: its reciprocal (used if it wins) formed off the serial path
         const C x0 = r[k];
-        const bool big = hypot(x0.x, x0.y) >= Lim<R>::sfmin();
+        const bool big = cbig(x0);
         const C rc = big ? crcp(x0) : x0;
         int prow = k;
         if(PIVOT)
@@ -332,6 +364,233 @@ static rocblas_status cx_getrf_warp(cudaStream_t s, int m, int n, Batch<C> A, in
     else
         cgetrf_warp_kernel<C, NMAX, false><<<grid, 32 * CPX_WPB, 0, s>>>(m, n, A, lda, ipiv, sP,
                                                                          info, bc, g);
+    return cudaGetLastError() == cudaSuccess ? rocblas_status_success
+                                             : rocblas_status_internal_error;
+}
+
+// ---- m, n <= 64, not both <= 32: one CTA per member, the whole member in registers.  Warp g
+// holds columns g*NC .. g*NC+NC-1 and lane i rows i and i+32 (S slots).  Rows stay where they
+// are and are relabelled (myrow = the row's current position), as in the warp kernel.  Per
+// column k one CTA barrier: before it the warp holding column k searches it, scales it by the
+// pivot's reciprocal and publishes the multipliers and the pivot (double-buffered by the
+// parity of k); after it every warp right of the column takes the pivot row's part of its own
+// columns from the pivot lane (warp-private shared memory, ordered by __syncwarp) and updates
+// its rows, and the warp holding column k+1 searches that next.
+template <typename C>
+struct CxRegPiv
+{
+    C pv, rcp;
+    int slot, label, big;
+};
+
+// search, pivot and scale column kc of the calling warp: v[s] holds the column's entry of row
+// lane + 32 s and takes its multiplier; the multipliers go to col (by slot), the pivot to pr
+template <typename C, int S, bool PIVOT>
+__device__ __forceinline__ void cx_reg_pivot(int kc, int m, C (&v)[S], const int (&myrow)[S],
+                                             CxRegPiv<C>& pr, C* col, int* piv)
+{
+    using R = typename CxReal<C>::R;
+    using K = typename KeyOf<R>::type;
+    const int lane = threadIdx.x & 31;
+    K bk = 0;
+    int bl = INT_MAX, bs = 0;
+#pragma unroll
+    for(int s = 0; s < S; ++s)
+    {
+        const bool ok = lane + 32 * s < m && (PIVOT ? myrow[s] >= kc : myrow[s] == kc);
+        const K key = pivot_key((R)(fabs(v[s].x) + fabs(v[s].y)), myrow[s] == kc);
+        if(ok && (bl == INT_MAX || key > bk || (key == bk && myrow[s] < bl)))
+        {
+            bk = key;
+            bl = myrow[s];
+            bs = s;
+        }
+    }
+    // this lane's reciprocal, formed while the warp reduction runs
+    const C bv = bs == 0 ? v[0] : v[S - 1];
+    const bool big = cbig(bv);
+    const C rc = big ? crcp(bv) : bv;
+    const int p = warp_argmax_fast(bk, bl, bl != INT_MAX); // row kc is always a candidate
+    if(bl == p)
+    {
+        pr.pv = bv;
+        pr.rcp = rc;
+        pr.big = big;
+        pr.slot = lane + 32 * bs;
+        pr.label = p;
+        if(PIVOT)
+            piv[kc] = p + 1;
+    }
+    __syncwarp();
+    const C pv = pr.pv, r = pr.rcp;
+    const bool pb = pr.big != 0;
+    const int slot = pr.slot;
+#pragma unroll
+    for(int s = 0; s < S; ++s)
+        if(lane + 32 * s < m && myrow[s] >= kc && lane + 32 * s != slot)
+        {
+            // LAPACK zgetf2: reciprocal when |pivot| >= sfmin, else division; a zero pivot
+            // leaves the column unscaled
+            C l = v[s];
+            if(!czero(pv))
+                l = pb ? cmul(l, r) : cdiv(l, pv);
+            v[s] = l;
+            col[lane + 32 * s] = l;
+        }
+}
+
+template <typename C, int NC, int S, bool PIVOT>
+__global__ void __launch_bounds__(32 * (64 / NC), 2)
+    cgetrf_reg_kernel(int m, int n, Batch<C> A, int lda, int* ipiv, int64_t strideP, int* info,
+                      Gate gate)
+{
+    constexpr int G = 64 / NC;
+    __shared__ CxRegPiv<C> spiv[2];
+    __shared__ C scol[2][32 * S];
+    __shared__ C sprow[G][NC];
+    const int64_t b = blockIdx.x;
+    if(gate.skip(b))
+        return;
+    C* a = A.at(b);
+    int* piv = PIVOT ? ipiv + b * strideP : nullptr;
+    const int g = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    C r[S][NC];
+    int myrow[S];
+#pragma unroll
+    for(int s = 0; s < S; ++s)
+    {
+        myrow[s] = lane + 32 * s;
+#pragma unroll
+        for(int j = 0; j < NC; ++j)
+            r[s][j] = (lane + 32 * s < m && g * NC + j < n)
+                          ? RSB_AT(a, lane + 32 * s, g * NC + j, lda, m, n)
+                          : cx<C>(0, 0);
+    }
+    const int mn = min(m, n);
+    int inf = 0;
+    if(g == 0)
+    {
+        C v[S];
+#pragma unroll
+        for(int s = 0; s < S; ++s)
+            v[s] = r[s][0];
+        cx_reg_pivot<C, S, PIVOT>(0, m, v, myrow, spiv[0], scol[0], piv);
+#pragma unroll
+        for(int s = 0; s < S; ++s)
+            r[s][0] = v[s];
+    }
+    const int ng = (mn + NC - 1) / NC;
+    for(int g0 = 0; g0 < ng; ++g0)
+    {
+#pragma unroll
+        for(int kk = 0; kk < NC; ++kk)
+        {
+            const int k = g0 * NC + kk;
+            if(k < mn)
+            {
+                const int buf = k & 1;
+                __syncthreads();
+                const int ps = spiv[buf].slot, p = spiv[buf].label;
+                if(inf == 0 && czero(spiv[buf].pv))
+                    inf = k + 1;
+                if(PIVOT)
+#pragma unroll
+                    for(int s = 0; s < S; ++s)
+                        myrow[s] = myrow[s] == p ? k : (myrow[s] == k ? p : myrow[s]);
+                if(g >= g0)
+                {
+                    // the pivot row's part of this warp's columns right of k
+                    if(lane == (ps & 31))
+                    {
+#pragma unroll
+                        for(int j = 0; j < NC; ++j)
+                            if(g > g0 || j > kk)
+                                sprow[g][j] = (S == 1 || ps < 32) ? r[0][j] : r[S - 1][j];
+                    }
+                    __syncwarp();
+                    C l[S];
+                    bool act[S];
+#pragma unroll
+                    for(int s = 0; s < S; ++s)
+                    {
+                        act[s] = lane + 32 * s < m && myrow[s] > k;
+                        l[s] = act[s] ? scol[buf][lane + 32 * s] : cx<C>(0, 0);
+                    }
+                    if(g == g0)
+                    {
+#pragma unroll
+                        for(int j = kk + 1; j < NC; ++j)
+                        {
+                            const C u = sprow[g][j];
+#pragma unroll
+                            for(int s = 0; s < S; ++s)
+                                if(act[s])
+                                    r[s][j] = csub(r[s][j], cmul(l[s], u));
+                        }
+                    }
+                    else
+                    {
+#pragma unroll
+                        for(int j = 0; j < NC; ++j)
+                        {
+                            const C u = sprow[g][j];
+#pragma unroll
+                            for(int s = 0; s < S; ++s)
+                                if(act[s])
+                                    r[s][j] = csub(r[s][j], cmul(l[s], u));
+                        }
+                    }
+                }
+                // the next column's pivot, by the warp that holds it
+                if(k + 1 < mn)
+                {
+                    const int jn = (kk + 1) % NC;
+                    if(kk + 1 < NC ? g == g0 : g == g0 + 1)
+                    {
+                        C v[S];
+#pragma unroll
+                        for(int s = 0; s < S; ++s)
+                            v[s] = r[s][jn];
+                        cx_reg_pivot<C, S, PIVOT>(k + 1, m, v, myrow, spiv[buf ^ 1],
+                                                  scol[buf ^ 1], piv);
+#pragma unroll
+                        for(int s = 0; s < S; ++s)
+                            r[s][jn] = v[s];
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for(int s = 0; s < S; ++s)
+        if(lane + 32 * s < m)
+#pragma unroll
+            for(int j = 0; j < NC; ++j)
+                if(g * NC + j < n)
+                    RSB_AT(a, myrow[s], g * NC + j, lda, m, n) = r[s][j];
+    if(threadIdx.x == 0)
+        info[b] = inf;
+}
+
+template <typename C, int NC>
+static rocblas_status cx_getrf_reg(cudaStream_t s, int m, int n, Batch<C> A, int lda,
+                                   int* ipiv, int64_t sP, int* info, int bc, bool pivot, Gate g)
+{
+    constexpr int NT = 32 * (64 / NC);
+    if(m > 32)
+    {
+        if(pivot)
+            cgetrf_reg_kernel<C, NC, 2, true><<<bc, NT, 0, s>>>(m, n, A, lda, ipiv, sP, info, g);
+        else
+            cgetrf_reg_kernel<C, NC, 2, false><<<bc, NT, 0, s>>>(m, n, A, lda, ipiv, sP, info, g);
+    }
+    else
+    {
+        if(pivot)
+            cgetrf_reg_kernel<C, NC, 1, true><<<bc, NT, 0, s>>>(m, n, A, lda, ipiv, sP, info, g);
+        else
+            cgetrf_reg_kernel<C, NC, 1, false><<<bc, NT, 0, s>>>(m, n, A, lda, ipiv, sP, info, g);
+    }
     return cudaGetLastError() == cudaSuccess ? rocblas_status_success
                                              : rocblas_status_internal_error;
 }
@@ -820,6 +1079,11 @@ rocblas_status cx_getrf(cudaStream_t s, int m, int n, Batch<C> A, int lda, int* 
         if(mx <= 16)
             return cx_getrf_warp<C, 16>(s, m, n, A, lda, ipiv, sP, info, bc, pivot, g);
         return cx_getrf_warp<C, 32>(s, m, n, A, lda, ipiv, sP, info, bc, pivot, g);
+    }
+    if(m <= 64 && n <= 64)
+    {
+        RSB_LOG_KERNEL("cgetrf_reg_kernel");
+        return cx_getrf_reg<C, 8>(s, m, n, A, lda, ipiv, sP, info, bc, pivot, g);
     }
     const size_t bytes = sizeof(C) * (size_t)m * n;
     if(bytes <= CPX_SMEM_MAX)

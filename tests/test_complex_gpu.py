@@ -431,6 +431,48 @@ def test_warp_lu_small_shapes(handle, P, m, n, pivot):
 
 
 @pytest.mark.parametrize("P", ["c", "z"])
+@pytest.mark.parametrize("m,n", [(33, 33), (64, 64), (64, 33), (33, 64), (20, 64), (64, 20),
+                                 (40, 63), (57, 48)])
+@pytest.mark.parametrize("pivot", [True, False])
+def test_register_lu_shapes(handle, P, m, n, pivot):
+    """The register-resident LU (m, n <= 64, not both <= 32; one CTA per member, warps over
+    column groups): rectangular shapes either way, one or two rows per lane, padded leading
+    dimension, with and without pivoting, against the oracle."""
+    A = uniform_complex(m, n, 6, seed=m * 67 + n).astype(DT[P])
+    if not pivot:
+        for b in range(6):
+            A[b][np.arange(min(m, n)), np.arange(min(m, n))] += 8.0
+    LU, ipiv, info = gpu_getrf(handle, P, A, pivot=pivot, lda=m + 3)
+    oLU, oipiv, oinfo = oracle_getrf(A, pivot=pivot)
+    np.testing.assert_array_equal(info, oinfo)
+    if pivot:
+        np.testing.assert_array_equal(ipiv, oipiv)
+    for b in range(6):
+        assert norm_error("F", oLU[b], LU[b]) <= 4 * max(m, n) * eps(P)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
+def test_register_lu_nan_zero_and_ties(handle, P):
+    """n = 48 (register LU): a NaN in the first candidate row wins, one elsewhere never does;
+    a zero column sets info and the factorisation goes on; equal magnitudes pick the first
+    row in position order (LAPACK izamax) after earlier interchanges."""
+    n = 48
+    A = uniform_complex(n, n, 4, seed=77).astype(DT[P])
+    A[0][0, 0] = complex(np.nan, 0)
+    A[1][40, 0] = complex(0, np.nan)
+    A[2][:, 35] = 0
+    A[3][:, :] = np.round(A[3] * 2) / 2  # many exact ties in |re| + |im|
+    LU, ipiv, info = gpu_getrf(handle, P, A)
+    oLU, oipiv, oinfo = oracle_getrf(A)
+    np.testing.assert_array_equal(ipiv[:, :1], oipiv[:, :1])
+    np.testing.assert_array_equal(info, oinfo)
+    assert info[2] == 36
+    for b in (2, 3):
+        np.testing.assert_array_equal(ipiv[b], oipiv[b])
+        assert norm_error("F", oLU[b], LU[b]) <= n * eps(P)
+
+
+@pytest.mark.parametrize("P", ["c", "z"])
 @pytest.mark.parametrize("n", [1, 5, 17, 32])
 @pytest.mark.parametrize("lower", [True, False])
 def test_warp_cholesky_small(handle, P, n, lower):
