@@ -920,11 +920,12 @@ def run_wide(name, args, ctx, steps, warmup, cpu_seconds):
                           "timed events"}
         w.bytes_per_unit = 2 * n * n * es + 4 * n + 4        # zgetrf: A in and out, ipiv, info
         w.flops_per_unit = 8.0 * n ** 3 / 3 + 8.0 * n * n * nrhs
-        w.kernel = "cgetrf_smem_kernel<rocblas_double_complex> (member in shared memory)"
-        # 211.2 MB per 2048 members from `ncu --set full --clock-control none -k
-        # regex:cgetrf_smem -c 1 python -m rocsolver_b200.demo --case getrf --dtype z --n 64
+        w.kernel = ("cgetrf_reg_kernel<rocblas_double_complex, 8, 2, true> (member in "
+                    "registers, one CTA barrier per column)")
+        # 217.1 MB per 2048 members from `ncu --set full --clock-control none -k
+        # regex:cgetrf_reg -c 1 python -m rocsolver_b200.demo --case getrf --dtype z --n 64
         # --batch 2048 --reps 2`
-        w.traffic_per_unit = (134246144 + 76958208) / 2048
+        w.traffic_per_unit = (134357248 + 82747648) / 2048
         A_, B_ = w.A0.clone(), w.B0.clone()
         ipiv = torch.zeros(bc * n, dtype=torch.int32, device=dev)
         info = torch.zeros(bc, dtype=torch.int32, device=dev)
@@ -1087,7 +1088,8 @@ def run_wide(name, args, ctx, steps, warmup, cpu_seconds):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "pipeline": sl.desc},
             "roofline": {"bound": "hbm",
-                         "limiter": "instructions and per-column barriers of one CTA per member"
+                         "limiter": "latency: the per-column pivot chain of the warp holding "
+                                    "the column, 2 members (16 warps) per SM"
                          if name == "zgesv_n64" else
                          "latency: dependent dot-product chains in shared memory, 12 warps/SM",
                          "kernel": w.kernel, "achieved": gbs, "peak": peaks["hbm_gbs"],

@@ -7,9 +7,10 @@
 // substitution) and Hermitian Cholesky (roclapack_potf2.hpp:185-248 with conjugated dots).
 //
 // Design.  getrf: m, n <= 32 one warp per member with rows in registers
-// (cgetrf_warp_kernel); members up to 96 KB one CTA per member factoring a shared-memory copy
-// (cgetrf_smem_kernel); larger members the same device code in place in global memory
-// (cgetrf_kernel).  Per column: the pivot is the first largest |re| + |im| (LAPACK izamax; a
+// (cgetrf_warp_kernel); m, n <= 64 one CTA per member with the member in registers, warps
+// over column groups (cgetrf_reg_kernel); other members up to 96 KB one CTA per member
+// factoring a shared-memory copy (cgetrf_smem_kernel); larger members the same device code
+// in place in global memory (cgetrf_kernel).  Per column: the pivot is the first largest |re| + |im| (LAPACK izamax; a
 // NaN only wins in the first position, through the same pivot keys as the real kernels), rows
 // are interchanged over all columns, the column is scaled by the reciprocal (|pivot| >=
 // sfmin) or by division, and the trailing matrix takes the rank-1 update.  potrf: the same
