@@ -380,8 +380,8 @@ static rocblas_status cx_getrf_warp(cudaStream_t s, int m, int n, Batch<C> A, in
 template <typename C>
 struct CxRegPiv
 {
-    C pv, rcp;
-    int slot, label, big;
+    C pv;
+    int slot, label;
 };
 
 // search, pivot and scale column kc of the calling warp: v[s] holds the column's entry of row
@@ -407,24 +407,20 @@ __device__ __forceinline__ void cx_reg_pivot(int kc, int m, C (&v)[S], const int
             bs = s;
         }
     }
-    // this lane's reciprocal, formed while the warp reduction runs
-    const C bv = bs == 0 ? v[0] : v[S - 1];
-    const bool big = cbig(bv);
-    const C rc = big ? crcp(bv) : bv;
     const int p = warp_argmax_fast(bk, bl, bl != INT_MAX); // row kc is always a candidate
     if(bl == p)
     {
-        pr.pv = bv;
-        pr.rcp = rc;
-        pr.big = big;
+        pr.pv = bs == 0 ? v[0] : v[S - 1];
         pr.slot = lane + 32 * bs;
         pr.label = p;
         if(PIVOT)
             piv[kc] = p + 1;
     }
     __syncwarp();
-    const C pv = pr.pv, r = pr.rcp;
-    const bool pb = pr.big != 0;
+    // every lane forms the same reciprocal of the broadcast pivot
+    const C pv = pr.pv;
+    const bool pb = cbig(pv);
+    const C r = pb ? crcp(pv) : pv;
     const int slot = pr.slot;
 #pragma unroll
     for(int s = 0; s < S; ++s)
