@@ -436,8 +436,9 @@ __device__ __forceinline__ void cx_reg_pivot(int kc, int m, C (&v)[S], const int
         }
 }
 
+// complex float members fit three CTAs per SM (80 registers), complex double two
 template <typename C, int NC, int S, bool PIVOT>
-__global__ void __launch_bounds__(32 * (64 / NC), 2)
+__global__ void __launch_bounds__(32 * (64 / NC), sizeof(C) == 8 ? 3 : 2)
     cgetrf_reg_kernel(int m, int n, Batch<C> A, int lda, int* ipiv, int64_t strideP, int* info,
                       Gate gate)
 {
